@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Benchmark: walker-steps/s and NS iterations/s of the B200 NS walk.
+
+Workload (the batched-replica LJ configuration): 32-atom LJ NPT (eps=sigma=1,
+rc=2.5), P=8 runs at pressures log-spaced 0.01-1.0, K=512 walkers each,
+n_mcmc_steps=40, galilean (n_reflect=10, step 0.1, weight 4) + volume (step
+0.3, weight 1), pressure replica exchange every 10 iterations; uniform-gas
+start (cubic cell, V ~ U(0, 8N], fractional coordinates U[0,1)^3) from a
+seeded threefry key.  All inputs synthetic.
+
+One step = one launch of 10 NS iterations on all 8 runs (the iterations
+between two replica-exchange passes) + the swap pass.  walker-steps/s =
+P * (n_cull + n_extra) * n_mcmc_steps * iterations / s.
+
+``--impl reference`` times the reference's algorithm on the host CPU: the
+CPU oracle in the reference's own float32 arithmetic (JAX is not installable
+here), threaded over the runs.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+P_RUNS, K, N, T, R_REFLECT, RE_INTERVAL = 8, 512, 32, 40, 10, 10
+PRESSURES = np.logspace(-2, 0, P_RUNS).astype(np.float32)
+METRIC = "walker-steps/s"
+CONFIG = {
+    "workload": "LJ-32 NPT, 8 pressure replicas (0.01-1.0) x 512 walkers, "
+                "n_mcmc_steps=40, galilean(n_reflect=10)+volume, RE every 10 iterations",
+    "n_runs": P_RUNS, "n_walkers": K, "n_atoms": N, "n_mcmc_steps": T,
+    "n_reflect": R_REFLECT, "re_interval": RE_INTERVAL, "n_cull": 1, "n_extra": 0,
+    "iterations_per_step": RE_INTERVAL,
+}
+# algorithmic flops per unique pair interaction (triclinic MIC accounting)
+FLOPS_EF, FLOPS_E = 61.0, 48.0
+
+
+def build_case(seed: int):
+    from jaxrens_b200 import EnsembleTerm, Hamiltonian, build_mwg, create_lj, prng
+    from jaxrens_b200 import init as jinit
+    from jaxrens_b200 import moves as mvs
+
+    lj = create_lj(epsilon=1.0, sigma=1.0, cutoff=2.5)
+    H = Hamiltonian(lj, [EnsembleTerm(pressure=0.1)])
+    moves = [mvs.gmc(n_reflect=R_REFLECT, step_size=0.1, weight=4.0),
+             mvs.volume_move(N, step_size=0.3, weight=1.0)]
+    init_fn, step, _ = build_mwg(H, moves)
+    root = prng.key(seed)
+    keys = prng.split(root, P_RUNS + 2)
+    pos, cells = [], []
+    for r in range(P_RUNS):
+        p_, c_ = jinit.uniform_gas(keys[r], K, N, 8.0 * N)
+        pos.append(p_)
+        cells.append(c_)
+    types = [np.zeros((K, N), np.int32) for _ in range(P_RUNS)]
+    run_keys = prng.split(keys[P_RUNS], P_RUNS)
+    return H, init_fn, step, pos, cells, types, run_keys, keys[P_RUNS + 1]
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fp32_peak_tflops(torch) -> float:
+    """Measured FP32 FMA-pipe throughput (probe kernel, best of 5)."""
+    from jaxrens_b200 import _lib
+
+    L = _lib.load()
+    dev = torch.device("cuda")
+    scratch = torch.zeros(148 * 64, dtype=torch.float32, device=dev)
+    fl = C.c_double(0.0)
+    s = torch.cuda.current_stream().cuda_stream
+    blocks = 148 * 8
+    _lib.check(L.jr_bench_fma_peak(blocks, 2000, C.c_void_p(scratch.data_ptr()), C.byref(fl), s), "fma")
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.check(L.jr_bench_fma_peak(blocks, 2000, C.c_void_p(scratch.data_ptr()), C.byref(fl), s), "fma")
+        e1.record()
+        e1.synchronize()
+        best = max(best, fl.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    return best
+
+
+def algorithmic_flops(info) -> float:
+    """Sum over the launch's committed iterations of eval counts x unique
+    pairs x flops per pair (61 energy+forces, 48 energy-only)."""
+    pairs = N * (N - 1) / 2.0
+    ne = info.n_evaluations.sum().item()
+    ng = info.n_grad_evaluations.sum().item()
+    return (ng * FLOPS_EF + (ne - ng) * FLOPS_E) * pairs
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from jaxrens_b200 import _lib, prng
+    from jaxrens_b200 import nested_sampling as nsm
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+
+    H, init_fn, step, pos, cells, types, run_keys, re_key = build_case(args.seed + 1000 * rank)
+    pr = {"pressure": PRESSURES}
+    ns = nsm.init_ns_parallel(init_fn, pos, types, None, cells, run_keys, ensemble_params=pr)
+    re = nsm.InterREManager(RE_INTERVAL, 1, re_key)
+    cfg = None
+    if args.tune:
+        best = _lib.JrLaunchConfig()
+        dims = nsm.make_dims(ns, step, T, 0)
+        la = nsm.prior_mass.log_alpha(K, 1)
+        params = step.with_evidence(la, float(nsm.prior_mass.iteration_offsets(K, 1)[1][0]))
+        sb = nsm.state_buffers(ns)
+        _lib.check(_lib.load().jr_autotune(C.byref(dims), C.byref(params), C.byref(sb), 10,
+                                           C.byref(best), torch.cuda.current_stream().cuda_stream),
+                   "jr_autotune")
+        cfg = best
+    elif args.cluster is not None:
+        cfg = _lib.JrLaunchConfig(args.threads, args.tpa, args.cluster)
+    # prologue: leave the random-gas start before measuring (untimed)
+    info = nsm.InfoBuffers(ns, step.n_moves, RE_INTERVAL, dead=True)
+    for _ in range(args.prologue // RE_INTERVAL):
+        nsm.ns_iterate(ns, step, RE_INTERVAL, T, 0, info=info, cfg=cfg)
+        re.apply(ns, step)
+    torch.cuda.synchronize()
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def one_step(record):
+        if record is not None:
+            record[0].record()
+        nsm.ns_iterate(ns, step, RE_INTERVAL, T, 0, info=info, cfg=cfg)
+        if record is not None:
+            record[1].record()
+        re.apply(ns, step)
+
+    for _ in range(args.warmup):
+        one_step(None)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    flops = 0.0
+    it_start = ns.iteration.clone()
+    for k in range(args.steps):
+        flush.fill_(float(k))  # evict the (L2-resident) walker state between steps
+        evs[k][0].record()
+        one_step(ev[k])
+        evs[k][1].record()
+        torch.cuda.synchronize()
+        flops += algorithmic_flops(info)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    kern_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(step_ms))
+    iters = int((ns.iteration - it_start)[0].item())
+    assert iters == args.steps * RE_INTERVAL
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    walker_steps = world * P_RUNS * 1 * T * iters
+    value = walker_steps / (total_ms * 1e-3)
+    ns_iters = world * P_RUNS * iters / (total_ms * 1e-3)
+    achieved = flops / (sum(kern_ms) * 1e-3) / 1e12
+    peak = fp32_peak_tflops(torch)
+
+    # ---- end to end: host state in, result out, through the public API ----
+    e2e = end_to_end(args, ns, step, re, cfg, torch, nsm)
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    cpu = cpu_baseline(args) if (world == 1 and not args.no_cpu) else None
+    line = {
+        "metric": METRIC, "value": value, "unit": "walker-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 pair terms, f64 accumulation", "data": "synthetic",
+        "config": dict(CONFIG, parallelism=f"replicas x{world} GPUs",
+                       l2="flushed (256 MiB write) between timed steps",
+                       launch=None if cfg is None else {"threads": cfg.threads, "tpa": cfg.tpa,
+                                                         "cluster": cfg.cluster}),
+        "ns_iters_per_s": ns_iters, "ns_iters_per_s_per_run": ns_iters / (world * P_RUNS),
+        "e2e": e2e,
+        "gpu_launches": 2 * args.steps,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak > 0 else None, "traffic": None,
+                     "peak_source": "measured FP32 FMA probe (jr_bench_fma_peak) on this GPU",
+                     "peak_nominal": 148 * 128 * 2 * 1.965e-3,
+                     "kernel": "ns_iterate_kernel", "flops_per_step": flops / args.steps},
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+
+
+def end_to_end(args, ns, step, re, cfg, torch, nsm):
+    """Each step: pinned-host state -> device, 10 iterations + swap through
+    the public API, per-iteration results (dead energies, log Z) -> host."""
+    pop = ns.population
+    fields = [pop.positions, pop.direction, pop.types, pop.energy, pop.energy64, pop.cell,
+              pop.step_sizes, pop.n_accepted, pop.n_proposed, ns.rng_key, ns.log_evidence,
+              ns.iteration, ns.emax]
+    host = [f.detach().cpu().pin_memory() for f in fields]
+    h2d = sum(h.numel() * h.element_size() for h in host)
+    info = nsm.InfoBuffers(ns, step.n_moves, RE_INTERVAL, dead=False)
+    out_e = torch.empty((RE_INTERVAL, P_RUNS), dtype=torch.float64).pin_memory()
+    out_z = torch.empty((RE_INTERVAL, P_RUNS), dtype=torch.float64).pin_memory()
+    d2h = out_e.numel() * 8 + out_z.numel() * 8
+    n = max(3, args.steps // 2)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(n):
+        for f, h in zip(fields, host):
+            f.copy_(h, non_blocking=True)
+        nsm.ns_iterate(ns, step, RE_INTERVAL, T, 0, info=info, cfg=cfg)
+        re.apply(ns, step)
+        out_e.copy_(info.emax, non_blocking=True)
+        out_z.copy_(info.log_evidence, non_blocking=True)
+    t1.record()
+    t1.synchronize()
+    ms = t0.elapsed_time(t1)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    return {"value": world * P_RUNS * T * RE_INTERVAL * n / (ms * 1e-3), "unit": "walker-steps/s",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": n}
+
+
+def _oracle_reference_run(seed: int, n_iter: int, threads: int):
+    """The reference algorithm on host cores (float32, reference op order)."""
+    from jaxrens_b200 import prior_mass
+    from oracle import oracle as O
+    from tests._cases import oracle_model, oracle_moves
+
+    H, init_fn, step, pos, cells, types, run_keys, _ = build_case(seed)
+    model, moves = oracle_model(H), oracle_moves(step)
+    reps = []
+    for r in range(P_RUNS):
+        e = np.array([O.energy(model, pos[r][k], types[r][k], cells[r][k],
+                               pressure=float(PRESSURES[r]), mode=O.REF32, forces=False)[0]
+                      for k in range(K)])
+        reps.append(O.Replica(pos[r], types[r], e, cells[r],
+                              np.tile(step.default_step_sizes, (K, 1)), run_keys[r],
+                              pressure=float(PRESSURES[r])))
+    la = prior_mass.log_alpha(K, 1)
+    wo = float(prior_mass.iteration_offsets(K, 1)[1][0])
+    # prologue past the random-gas start, then the timed sample
+    for _ in range(5):
+        O.ns_step_batched(model, moves, reps, T, la, wo, shared_move_key=True,
+                          mode=O.REF32, n_threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(n_iter):
+        O.ns_step_batched(model, moves, reps, T, la, wo, shared_move_key=True,
+                          mode=O.REF32, n_threads=threads)
+    dt = time.perf_counter() - t0
+    return P_RUNS * T * n_iter / dt, dt
+
+
+def cpu_baseline(args):
+    threads = min(os.cpu_count() or 1, P_RUNS)
+    val, dt = _oracle_reference_run(args.seed, args.cpu_iters, threads)
+    return {"value": val, "unit": "walker-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{args.cpu_iters} NS iterations x {P_RUNS} runs (after 5 untimed), "
+                      f"{dt:.1f} s, CPU oracle in the reference's float32 op order"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = min(os.cpu_count() or 1, P_RUNS)
+    vals = []
+    for _ in range(max(1, args.steps)):
+        v, _ = _oracle_reference_run(args.seed, max(1, args.cpu_iters // max(1, args.steps)), threads)
+        vals.append(v)
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "walker-steps/s",
+        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": dict(CONFIG, parallelism=f"{threads} host threads over runs"),
+        "cpu_baseline": {"value": value, "unit": "walker-steps/s", "cores": threads,
+                         "kind": "port",
+                         "sample": "reference algorithm (CPU oracle, reference float32 op order); "
+                                   "JAX is not installable on this image"},
+        "e2e": {"value": value, "unit": "walker-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--prologue", type=int, default=200)
+    ap.add_argument("--cpu-iters", type=int, default=40)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tune", action="store_true")
+    ap.add_argument("--cluster", type=int, default=None)
+    ap.add_argument("--threads", type=int, default=256)
+    ap.add_argument("--tpa", type=int, default=8)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

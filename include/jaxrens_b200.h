@@ -1,0 +1,228 @@
+/*
+ * jaxrens_b200.h -- C-ABI of the B200 nested-sampling walk.
+ *
+ * Drop-in boundary for jaxrens's jitted NS iteration.  Every buffer is a
+ * device pointer owned by the caller (XLA, torch, or plain CUDA); the library
+ * allocates nothing on the call path.  All entry points are asynchronous on
+ * the given stream and return 0 on success or a negative JR_ERR_* code, with
+ * a message available from jr_last_error().
+ *
+ * Reference interfaces replaced (paths inside the jaxrens source tree):
+ *   jr_ns_iterate      <- the jit'd ns_step that _run_loop calls,
+ *                         src/jaxrens/sampling/run_loop.py:416-421 and :511-516
+ *                         (ns_step, src/jaxrens/sampling/nested_sampling.py:391-686,
+ *                         batched by src/jaxrens/sampling/batch_descriptor.py:177-195)
+ *   jr_move_trial      <- per_move_fns[k] (src/jaxrens/sampling/mwg.py:152-154),
+ *                         used by adjust_step_size
+ *                         (src/jaxrens/sampling/adaptation/stepsize_handler.py:246-255)
+ *                         and the burn-in walk (src/jaxrens/init/burn_in.py:48-151)
+ *   jr_energy_forces   <- eval_energy_and_forces on Hamiltonian(LJBackend, EnsembleTerm)
+ *                         (src/jaxrens/backends/base.py:74-113,
+ *                          src/jaxrens/backends/hamiltonian.py:112-153,
+ *                          src/jaxrens/backends/lj.py:125-204,
+ *                          src/jaxrens/backends/ensemble.py:34-59)
+ *   jr_re_swap         <- replica_exchange_step with EnsembleSwap
+ *                         (src/jaxrens/sampling/moves/replica_exchange.py:318-436),
+ *                         fired by InterREManager.apply
+ *                         (src/jaxrens/sampling/inter_re_manager.py:225-273)
+ *
+ * Layout (structure-of-arrays, mirroring the MCState leaves of
+ * src/jaxrens/state/mc_state.py:70-95 with a leading replica axis P and a
+ * padded atom axis Nmax; rows of `cell` are lattice vectors and positions are
+ * row vectors, as in src/jaxrens/utils/cell.py):
+ *   positions  float [P][K][Nmax][3]     direction float [P][K][Nmax][3]
+ *   types      int32 [P][K][Nmax]        cell      float [P][K][3][3]
+ *   energy     float [P][K] (float32 view of energy64)
+ *   energy64   double[P][K] (full ensemble potential U + P*V - mu*N)
+ *   step_sizes float [P][K][M]           n_accepted/n_proposed int32 [P][K][M]
+ *   rng_key    uint32[P][2] (jax.random.key_data words)
+ *   log_evidence double[P]  iteration int32[P]  emax double[P]
+ *   n_atoms int32[P]  pressure float[P]  mu float[P][S] (or NULL)
+ */
+#ifndef JAXRENS_B200_H
+#define JAXRENS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JR_MAX_SPECIES 8
+#define JR_MAX_MOVES 8
+#define JR_MAX_IMAGES 125
+#define JR_MAX_CENTERS 8
+#define JR_MAX_ATOMS 256
+
+enum {
+  JR_OK = 0,
+  JR_ERR_SHAPE = -1,       /* inconsistent or unsupported dimensions */
+  JR_ERR_PARAM = -2,       /* invalid parameter value */
+  JR_ERR_CUDA = -3,        /* a CUDA runtime call failed */
+  JR_ERR_TIMEOUT = -4,     /* a bounded device-side wait gave up */
+  JR_ERR_WORKSPACE = -5,   /* workspace missing or too small */
+  JR_ERR_UNSUPPORTED = -6  /* feature outside this build (e.g. n_cull > 1) */
+};
+
+enum { JR_MODEL_LJ = 0, JR_MODEL_GAUSS_MIX = 1 };
+enum { JR_MOVE_GALILEAN = 0, JR_MOVE_VOLUME = 1, JR_MOVE_MORPH = 2,
+       JR_MOVE_SWAP = 3 };
+
+typedef struct JrDims {
+  int32_t n_replicas;      /* P */
+  int32_t n_walkers;       /* K */
+  int32_t n_atoms_max;     /* Nmax (padding stride of the atom axis) */
+  int32_t n_moves;         /* M */
+  int32_t n_mcmc_steps;    /* T */
+  int32_t n_extra;         /* extra walked survivors per iteration */
+  int32_t n_cull;          /* culled walkers per iteration (this build: 1) */
+  int32_t shared_move_key; /* 1: move schedule from fold_in(rng_key[0], 1)
+                              (VmapRuns); 0: from each run's own key */
+} JrDims;
+
+/* Energy model: LJ with per-species-pair tables (or the Gaussian-mixture
+ * validation toy).  Tables are row-major S x S, already in the float32 form
+ * the reference evaluates: eps4 = f32(4*eps_ij), eps24 = f32(24*eps_ij),
+ * sig2 = f32(sigma_ij**2). */
+typedef struct JrModelParams {
+  int32_t model;
+  int32_t n_species;
+  int32_t has_cutoff;
+  float rc2;
+  float eps4[JR_MAX_SPECIES * JR_MAX_SPECIES];
+  float eps24[JR_MAX_SPECIES * JR_MAX_SPECIES];
+  float sig2[JR_MAX_SPECIES * JR_MAX_SPECIES];
+  int32_t n_images;                  /* supercell image offsets, (0,0,0) included */
+  float img_off[JR_MAX_IMAGES * 3];
+  int32_t n_centers;
+  float centers[JR_MAX_CENTERS * 3];
+  float gm_sigma;
+} JrModelParams;
+
+typedef struct JrMoveParams {
+  int32_t n_moves;
+  int32_t type[JR_MAX_MOVES];        /* JR_MOVE_* */
+  int32_t n_reflect[JR_MAX_MOVES];   /* galilean */
+  float perturb_angle[JR_MAX_MOVES]; /* galilean */
+  float cum_probs[JR_MAX_MOVES];     /* float32 cumsum(w / sum(w)) */
+  float max_vpa, min_vpa, min_aspect; /* cell-geometry guard */
+  int32_t flat_v_prior;
+} JrMoveParams;
+
+typedef struct JrParams {
+  JrModelParams model;
+  JrMoveParams moves;
+  double log_alpha;  /* log((K+1-n_cull)/(K+1)) */
+  double w_offset;   /* log dead weight offset of the iteration's cull */
+} JrParams;
+
+typedef struct JrStateBuffers {
+  float* positions;
+  float* direction;
+  int32_t* types;
+  float* energy;
+  double* energy64;
+  float* cell;
+  float* step_sizes;
+  int32_t* n_accepted;
+  int32_t* n_proposed;
+  uint32_t* rng_key;
+  double* log_evidence;
+  int32_t* iteration;
+  double* emax;
+  const int32_t* n_atoms;
+  const float* pressure;
+  const float* mu;      /* NULL when the ensemble has no chemical potentials */
+} JrStateBuffers;
+
+/* Per-iteration outputs of jr_ns_iterate, leading axis n_iter then P.
+ * Any pointer may be NULL to skip that output. */
+typedef struct JrInfoBuffers {
+  int32_t* worst_idx;              /* [n_iter][P] */
+  int32_t* clone_idx;              /* [n_iter][P] */
+  double* emax;                    /* [n_iter][P] */
+  double* log_evidence;            /* [n_iter][P] after the iteration */
+  float* dead_positions;           /* [n_iter][P][Nmax][3] */
+  int32_t* dead_types;             /* [n_iter][P][Nmax] */
+  float* dead_cell;                /* [n_iter][P][9] */
+  int32_t* n_accepted;             /* [n_iter][P][M] */
+  int32_t* n_proposed;             /* [n_iter][P][M] */
+  int32_t* reject_reason_counts;   /* [n_iter][P][M][4] */
+  int32_t* n_evaluations;          /* [n_iter][P][M] */
+  int32_t* n_grad_evaluations;     /* [n_iter][P][M] */
+  int32_t* rounds;                 /* [P] speculation rounds used (diagnostic) */
+} JrInfoBuffers;
+
+/* Launch shape of the walk kernels.  threads: CTA size; tpa: threads per
+ * atom in the pair loop (power of two <= 32); cluster: CTAs per replica
+ * (thread-block cluster) used for speculative iterations.  Results do not
+ * depend on the launch shape. */
+typedef struct JrLaunchConfig {
+  int32_t threads;
+  int32_t tpa;
+  int32_t cluster;
+} JrLaunchConfig;
+
+/* ---- NS iterations (replaces the jit'd ns_step) ---- */
+size_t jr_ns_iterate_workspace_size(const JrDims* dims);
+
+/* Runs n_iter NS iterations on every replica.  `cfg` may be NULL (cached
+ * autotune result for these dims, else a heuristic).  `workspace` is device
+ * memory of jr_ns_iterate_workspace_size(dims) bytes. */
+int jr_ns_iterate(const JrDims* dims, const JrParams* params,
+                  const JrStateBuffers* state, const JrInfoBuffers* info,
+                  int32_t n_iter, const JrLaunchConfig* cfg, void* workspace,
+                  size_t workspace_bytes, void* stream);
+
+/* ---- one move per (replica, trial) walker (adaptation / burn-in) ---- */
+/* walker_idx [P][n_trials], keys [P][n_trials][2], step [P], emax [P];
+ * accepted [P][n_trials].  write_back=1 stores the moved walkers in place
+ * (burn-in); write_back=0 only reports acceptance (step-size trials).
+ * move_idx < 0 draws the move from keys like the MWG step (using
+ * move_keys [P][n_trials][2]). */
+int jr_move_trial(const JrDims* dims, const JrParams* params,
+                  const JrStateBuffers* state, int32_t n_trials,
+                  int32_t move_idx, const int32_t* walker_idx,
+                  const uint32_t* keys, const uint32_t* move_keys,
+                  const float* step, const double* emax, int32_t write_back,
+                  int32_t* accepted, int32_t* reject_reason, void* stream);
+
+/* ---- energy + forces of a batch of configurations ---- */
+/* positions [B][Nmax][3], types [B][Nmax], cell [B][9], n_atoms [B],
+ * pressure [B], mu [B][S] or NULL; energy64 [B] (U + PV - mu N),
+ * energy_u [B] (U alone, may be NULL), forces [B][Nmax][3] (may be NULL). */
+int jr_energy_forces(const JrParams* params, int32_t n_configs,
+                     int32_t n_atoms_max, const float* positions,
+                     const int32_t* types, const float* cell,
+                     const int32_t* n_atoms, const float* pressure,
+                     const float* mu, double* energy64, double* energy_u,
+                     float* forces, void* stream);
+
+/* ---- pressure / semi-grand replica exchange pass ---- */
+/* key: the swap key words (host values).  acc/att_per_pair [P-1] (may be
+ * NULL). Walker-bound fields travel; run-bound fields stay. */
+int jr_re_swap(const JrDims* dims, const JrStateBuffers* state,
+               uint32_t key0, uint32_t key1, int32_t n_swap_cycles,
+               int32_t n_species, int32_t* acc_per_pair,
+               int32_t* att_per_pair, void* stream);
+
+/* ---- autotuner: times launch shapes on a scratch copy of `state` ---- */
+int jr_autotune(const JrDims* dims, const JrParams* params,
+                const JrStateBuffers* state, int32_t n_iter_probe,
+                JrLaunchConfig* best, void* stream);
+
+/* ---- measurement utility: FP32 FMA-pipe throughput probe ----
+ * Launches n_blocks x 256 threads of independent FMA chains; *flops receives
+ * the floating-point operations the launch performs (time it with events).
+ * No counterpart in the reference: it supplies the roofline denominator. */
+int jr_bench_fma_peak(int n_blocks, int iters, float* scratch, double* flops,
+                      void* stream);
+
+const char* jr_last_error(void);
+int jr_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,950 @@
+// jr_ns.cu -- B200 kernels and the C-ABI of the nested-sampling walk.
+//
+// Kernels
+//   ns_iterate_kernel  n_iter NS iterations for every replica in one launch.
+//                      A thread-block cluster of C CTAs serves one replica.
+//                      Each round predicts the culls of the next D iterations
+//                      (the PRNG stream is state independent, and the culled
+//                      walker of iteration i+d is the (d+1)-th highest energy
+//                      as long as the walkers written by iterations < d stay
+//                      below it), walks them concurrently, then commits the
+//                      longest prefix whose predictions hold.  Committed
+//                      results are exactly those of sequential ns_step calls.
+//   move_trial_kernel  one move on many walkers (adaptation trials, burn-in)
+//   energy_kernel      energy + forces of a batch of configurations
+//   re_swap_kernel     pressure / semi-grand replica-exchange pass
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+
+#include "../../include/jaxrens_b200.h"
+#include "jr_rng.cuh"
+#include "jr_walk.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace jr {
+
+constexpr int kMaxD = 16;          // speculative iterations per round
+constexpr int kMaxWalk = 256;      // D * (1 + n_extra) bound
+
+struct NsShared {
+  int worst[kMaxD];
+  int clone[kMaxD];
+  double e[kMaxD];
+  int spec[kMaxD];
+  Key kmcmc[kMaxD];
+  Key kmove[kMaxD];
+  int extras[kMaxWalk];
+  int wset[kMaxWalk];
+  int n_wset;
+  double res_E;                    // final energy of this CTA's chain
+  unsigned long long u64[2][kMaxWarps];
+  int flag[2][kMaxWarps];
+};
+
+__device__ __forceinline__ unsigned long long ord_double(double x) {
+  unsigned long long u = (unsigned long long)__double_as_longlong(x);
+  return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double unord_double(unsigned long long k) {
+  unsigned long long u = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double((long long)u);
+}
+
+// Block max of a u64 and OR of an int flag; uniform result in every thread.
+__device__ inline void block_max_u64(NsShared& ns, int& par, unsigned long long& v,
+                                     int& f) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+  for (int off = 16; off > 0; off >>= 1) {
+    unsigned long long o = __shfl_xor_sync(0xffffffffu, v, off);
+    v = o > v ? o : v;
+    f |= __shfl_xor_sync(0xffffffffu, f, off);
+  }
+  if (lane == 0) {
+    ns.u64[par][warp] = v;
+    ns.flag[par][warp] = f;
+  }
+  __syncthreads();
+  v = 0;
+  f = 0;
+  for (int q = 0; q < nw; ++q) {
+    v = ns.u64[par][q] > v ? ns.u64[par][q] : v;
+    f |= ns.flag[par][q];
+  }
+  par ^= 1;
+}
+
+__device__ __forceinline__ bool in_set(const int* set, int n, int k) {
+  for (int q = 0; q < n; ++q)
+    if (set[q] == k) return true;
+  return false;
+}
+
+// _find_worst_walker (nested_sampling.py:86-109) over the candidates not in
+// `excl`: jnp.max (NaN-propagating), then argmax of uniform noise among the
+// exact ties (first index on equal noise).
+__device__ void cull_select(NsShared& ns, int& par, const double* E, int K,
+                            const int* excl, int nexcl, Key kworst, int& worst,
+                            double& emax, bool& any_nan) {
+  unsigned long long best = 0;
+  int nanf = 0;
+  for (int k = threadIdx.x; k < K; k += blockDim.x) {
+    if (in_set(excl, nexcl, k)) continue;
+    const double x = E[k];
+    if (isnan(x)) {
+      nanf = 1;
+    } else {
+      const unsigned long long o = ord_double(x);
+      best = o > best ? o : best;
+    }
+  }
+  block_max_u64(ns, par, best, nanf);
+  any_nan = nanf != 0;
+  if (any_nan) {
+    emax = __longlong_as_double(0x7ff8000000000000ll);
+    worst = 0;
+    return;
+  }
+  emax = unord_double(best);
+  unsigned long long tb = 0;
+  int dummy = 0;
+  for (int k = threadIdx.x; k < K; k += blockDim.x) {
+    if (in_set(excl, nexcl, k)) continue;
+    if (E[k] == emax) {
+      const float nz = uniform01(bits32(kworst, (uint32_t)k));
+      const unsigned long long key =
+          ((unsigned long long)__float_as_uint(nz) << 32) | (0xFFFFFFFFu - (unsigned)k);
+      tb = key > tb ? key : tb;
+    }
+  }
+  block_max_u64(ns, par, tb, dummy);
+  worst = (int)(0xFFFFFFFFu - (unsigned)(tb & 0xFFFFFFFFull));
+}
+
+// _get_extra_indices (nested_sampling.py:112-133): the n_extra largest uniform
+// noises, worst and clone excluded, stable (lower index first on ties).
+__device__ void select_extras(NsShared& ns, int& par, float* noise, int K,
+                              int worst, int clone, Key kextra, int n_extra,
+                              int* out) {
+  for (int k = threadIdx.x; k < K; k += blockDim.x)
+    noise[k] = (k == worst || k == clone) ? -1.0f : uniform01(bits32(kextra, (uint32_t)k));
+  __syncthreads();
+  for (int e = 0; e < n_extra; ++e) {
+    unsigned long long tb = 0;
+    int dummy = 0;
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+      const float nz = noise[k];
+      if (nz < 0.0f) continue;
+      const unsigned long long key =
+          ((unsigned long long)__float_as_uint(nz) << 32) | (0xFFFFFFFFu - (unsigned)k);
+      tb = key > tb ? key : tb;
+    }
+    block_max_u64(ns, par, tb, dummy);
+    const int pick = (int)(0xFFFFFFFFu - (unsigned)(tb & 0xFFFFFFFFull));
+    if (threadIdx.x == 0) {
+      out[e] = pick;
+      noise[pick] = -1.0f;
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ double logaddexp(double a, double b) {
+  const double amax = a > b ? a : b;
+  const double delta = a - b;
+  if (isnan(delta)) return a + b;
+  return amax + log1p(exp(-fabs(delta)));
+}
+
+__device__ inline void walk_chain(const JrParams& P, Walker& w, int T, Key chain_key,
+                                  Key move_key, double emax, float pressure,
+                                  const float* mu) {
+  for (int t = 0; t < T; ++t)
+    mwg_step(P, w, split(chain_key, (uint32_t)t), split(move_key, (uint32_t)t), emax,
+             pressure, mu);
+  __syncthreads();
+}
+
+// Copy the about-to-be-culled walker of replica p into info row `row`.
+__device__ inline void write_dead(const JrDims& D, const JrStateBuffers& st,
+                                  const JrInfoBuffers& info, int row, int p, int slot,
+                                  int n) {
+  const int K = D.n_walkers, Nmax = D.n_atoms_max, Pn = D.n_replicas;
+  const size_t wb = (size_t)p * K + slot;
+  const size_t ib = (size_t)row * Pn + p;
+  if (info.dead_positions)
+    for (int q = threadIdx.x; q < 3 * n; q += blockDim.x)
+      info.dead_positions[ib * Nmax * 3 + q] = st.positions[wb * Nmax * 3 + q];
+  if (info.dead_types)
+    for (int q = threadIdx.x; q < n; q += blockDim.x)
+      info.dead_types[ib * Nmax + q] = st.types[wb * Nmax + q];
+  if (info.dead_cell)
+    for (int q = threadIdx.x; q < 9; q += blockDim.x)
+      info.dead_cell[ib * 9 + q] = st.cell[wb * 9 + q];
+  __syncthreads();
+}
+
+__device__ inline void copy_params(JrParams& dst, const JrParams& src) {
+  const int nw = (int)(sizeof(JrParams) / 4);
+  const uint32_t* s = reinterpret_cast<const uint32_t*>(&src);
+  uint32_t* d = reinterpret_cast<uint32_t*>(&dst);
+  for (int q = threadIdx.x; q < nw; q += blockDim.x) d[q] = s[q];
+}
+
+__global__ void __launch_bounds__(512)
+ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
+                  const JrInfoBuffers info, const int n_iter, const int tpa,
+                  const int C, const uint32_t* __restrict__ key0_base) {
+  extern __shared__ __align__(16) unsigned char dyn[];
+  __shared__ WalkShared ws;
+  __shared__ NsShared ns;
+  __shared__ JrParams P;
+  copy_params(P, Pg);
+  cg::cluster_group cluster = cg::this_cluster();
+  const int p = blockIdx.x / C;
+  const int c = blockIdx.x % C;
+  const int K = D.n_walkers, M = D.n_moves, T = D.n_mcmc_steps;
+  const int nx = D.n_extra, W = 1 + nx;
+  const int n = st.n_atoms[p];
+  const int Dmax = (C >= 2 * W) ? (C / W < kMaxD ? C / W : kMaxD) : 1;
+  WalkArrays arr = carve(dyn, D.n_atoms_max, Pg.model.n_images);
+  double* Epop = reinterpret_cast<double*>(dyn + walk_dyn_smem_bytes(D.n_atoms_max, Pg.model.n_images));
+  float* noise = reinterpret_cast<float*>(Epop + K);
+  Walker w{ws, arr, n, tpa, 0};
+  int par = 0;
+  __syncthreads();
+  load_tables(P, ws);
+  const float pressure = st.pressure[p];
+  const float* mu = st.mu ? st.mu + (size_t)p * P.model.n_species : nullptr;
+  Key key{st.rng_key[2 * p], st.rng_key[2 * p + 1]};
+  Key key0{key0_base[0], key0_base[1]};
+  int iter = st.iteration[p];
+  double logZ = st.log_evidence[p];
+  int committed = 0, rounds = 0;
+  while (committed < n_iter) {
+    const int Dr = (n_iter - committed) < Dmax ? (n_iter - committed) : Dmax;
+    for (int k = threadIdx.x; k < K; k += blockDim.x) Epop[k] = st.energy64[(size_t)p * K + k];
+    if (threadIdx.x == 0) ns.n_wset = 0;
+    __syncthreads();
+    // ---- predictions for iterations d < Dr (every CTA, identically) ----
+    Key kd = key, k0d = key0;
+    for (int d = 0; d < Dr; ++d) {
+      const Key ka = split(kd, 0u), kw = split(kd, 1u);
+      const Key kclone = split(ka, 1u), kextra = split(ka, 2u);
+      const Key kmcmc = split(ka, 3u), kmoves = split(ka, 4u);
+      int worst;
+      double emax;
+      bool any_nan;
+      cull_select(ns, par, Epop, K, ns.wset, ns.n_wset, kw, worst, emax, any_nan);
+      int clone = randint(kclone, 0, K - 1);
+      if (clone >= worst) clone += 1;
+      if (nx > 0) select_extras(ns, par, noise, K, worst, clone, kextra, nx, ns.extras + d * nx);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        bool sp = (d == 0);
+        if (d > 0) {
+          sp = ns.spec[d - 1] && !any_nan && !isnan(ns.e[d - 1]) &&
+               !in_set(ns.wset, ns.n_wset, clone);
+          for (int e = 0; e < nx && sp; ++e)
+            if (in_set(ns.wset, ns.n_wset, ns.extras[d * nx + e])) sp = false;
+        }
+        ns.spec[d] = sp ? 1 : 0;
+        ns.worst[d] = worst;
+        ns.clone[d] = clone;
+        ns.e[d] = emax;
+        ns.kmcmc[d] = kmcmc;
+        ns.kmove[d] = D.shared_move_key ? split(k0d, 1u) : kmoves;
+        ns.wset[ns.n_wset++] = worst;
+        for (int e = 0; e < nx; ++e) ns.wset[ns.n_wset++] = ns.extras[d * nx + e];
+      }
+      __syncthreads();
+      kd = split(ka, 0u);
+      k0d = advance_iteration(k0d);
+    }
+    // ---- walk ----
+    zero_chain_counters(ws);
+    if (threadIdx.x == 0) ns.res_E = 0.0;
+    __syncthreads();
+    if (Dmax == 1) {
+      for (int sidx = c; sidx < W; sidx += C) {
+        const int src = sidx == 0 ? ns.clone[0] : ns.extras[sidx - 1];
+        const int dst = sidx == 0 ? ns.worst[0] : src;
+        if (sidx == 0) write_dead(D, st, info, committed, p, ns.worst[0], n);
+        load_walker(P, D, st, w, p, src, sidx == 0);
+        walk_chain(P, w, T, split(ns.kmcmc[0], (uint32_t)sidx), ns.kmove[0], ns.e[0],
+                   pressure, mu);
+        store_walker(D, st, w, p, dst);
+      }
+    } else {
+      const int d = c / W, wi = c % W;
+      if (d < Dr && ns.spec[d]) {
+        const int src = wi == 0 ? ns.clone[d] : ns.extras[d * nx + wi - 1];
+        load_walker(P, D, st, w, p, src, wi == 0);
+        walk_chain(P, w, T, split(ns.kmcmc[d], (uint32_t)wi), ns.kmove[d], ns.e[d],
+                   pressure, mu);
+        if (threadIdx.x == 0) ns.res_E = ws.E;
+      }
+    }
+    __syncthreads();
+    __threadfence();
+    cluster.sync();
+    // ---- validation: longest prefix whose predicted culls hold ----
+    int nval = 1;
+    if (Dmax > 1) {
+      nval = 0;
+      for (int d = 0; d < Dr; ++d) {
+        bool ok = ns.spec[d] != 0;
+        for (int d2 = 0; d2 < d && ok; ++d2)
+          for (int w2 = 0; w2 < W && ok; ++w2) {
+            const double* r = cluster.map_shared_rank(&ns.res_E, d2 * W + w2);
+            if (!(*r < ns.e[d])) ok = false;
+          }
+        if (!ok) break;
+        ++nval;
+      }
+      const int d = c / W, wi = c % W;
+      if (d < nval) {
+        const int dst = wi == 0 ? ns.worst[d] : ns.extras[d * nx + wi - 1];
+        if (wi == 0) write_dead(D, st, info, committed + d, p, ns.worst[d], n);
+        store_walker(D, st, w, p, dst);
+      }
+    }
+    // ---- per-iteration info and replica scalars (CTA 0) ----
+    if (c == 0 && threadIdx.x == 0) {
+      int it = iter;
+      for (int d = 0; d < nval; ++d, ++it) {
+        const size_t ib = (size_t)(committed + d) * D.n_replicas + p;
+        const int r0 = Dmax == 1 ? 0 : d * W;
+        const int r1 = Dmax == 1 ? C : d * W + W;
+        for (int m = 0; m < M; ++m) {
+          int a = 0, pr = 0, ne = 0, ng = 0, rr[4] = {0, 0, 0, 0};
+          for (int r = r0; r < r1; ++r) {
+            WalkShared* rs = cluster.map_shared_rank(&ws, r);
+            a += rs->c_acc[m];
+            pr += rs->c_prop[m];
+            ne += rs->c_nev[m];
+            ng += rs->c_ngr[m];
+            for (int q = 0; q < 4; ++q) rr[q] += rs->c_rr[4 * m + q];
+          }
+          if (info.n_accepted) info.n_accepted[ib * M + m] = a;
+          if (info.n_proposed) info.n_proposed[ib * M + m] = pr;
+          if (info.n_evaluations) info.n_evaluations[ib * M + m] = ne;
+          if (info.n_grad_evaluations) info.n_grad_evaluations[ib * M + m] = ng;
+          if (info.reject_reason_counts)
+            for (int q = 0; q < 4; ++q) info.reject_reason_counts[(ib * M + m) * 4 + q] = rr[q];
+        }
+        const double lw = (double)it * P.log_alpha + P.w_offset;
+        logZ = logaddexp(logZ, lw - ns.e[d]);
+        if (info.worst_idx) info.worst_idx[ib] = ns.worst[d];
+        if (info.clone_idx) info.clone_idx[ib] = ns.clone[d];
+        if (info.emax) info.emax[ib] = ns.e[d];
+        if (info.log_evidence) info.log_evidence[ib] = logZ;
+      }
+    }
+    for (int d = 0; d < nval; ++d) {
+      key = advance_iteration(key);
+      key0 = advance_iteration(key0);
+    }
+    if (c == 0 && threadIdx.x == 0) {
+      st.emax[p] = ns.e[nval - 1];
+      st.iteration[p] = iter + nval;
+      st.log_evidence[p] = logZ;
+      st.rng_key[2 * p] = key.k0;
+      st.rng_key[2 * p + 1] = key.k1;
+    }
+    iter += nval;
+    committed += nval;
+    ++rounds;
+    __syncthreads();
+    __threadfence();
+    cluster.sync();
+  }
+  if (c == 0 && threadIdx.x == 0 && info.rounds) info.rounds[p] = rounds;
+}
+
+// ------------------------------------------------------------ trials ----
+__global__ void __launch_bounds__(512)
+move_trial_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
+                  const int n_trials, const int move_idx, const int* walker_idx,
+                  const uint32_t* keys, const uint32_t* move_keys, const float* step,
+                  const double* emax, const int write_back, int* accepted,
+                  int* reject_reason, const int tpa) {
+  extern __shared__ __align__(16) unsigned char dyn[];
+  __shared__ WalkShared ws;
+  __shared__ JrParams P;
+  copy_params(P, Pg);
+  const int p = blockIdx.x / n_trials;
+  const int t = blockIdx.x % n_trials;
+  const int n = st.n_atoms[p];
+  WalkArrays arr = carve(dyn, D.n_atoms_max, Pg.model.n_images);
+  Walker w{ws, arr, n, tpa, 0};
+  __syncthreads();
+  load_tables(P, ws);
+  const size_t tb = (size_t)p * n_trials + t;
+  const int slot = walker_idx[tb];
+  load_walker(P, D, st, w, p, slot, false);
+  const float pressure = st.pressure[p];
+  const float* mu = st.mu ? st.mu + (size_t)p * P.model.n_species : nullptr;
+  const Key key{keys[2 * tb], keys[2 * tb + 1]};
+  int idx = move_idx;
+  if (idx < 0) {
+    const Key mk{move_keys[2 * tb], move_keys[2 * tb + 1]};
+    idx = choice(mk, P.moves.cum_probs, P.moves.n_moves);
+  }
+  int reason = 0;
+  const bool acc = run_move(P, w, idx, key, step[p], emax[p], pressure, mu, reason);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    accepted[tb] = acc ? 1 : 0;
+    if (reject_reason) reject_reason[tb] = acc ? 0 : (reason > 1 ? reason : 1);
+    if (write_back) {
+      ws.w_prop[idx] += 1;
+      ws.w_acc[idx] += acc ? 1 : 0;
+    }
+  }
+  if (write_back) store_walker(D, st, w, p, slot);
+}
+
+// ------------------------------------------------------------ energy ----
+__global__ void __launch_bounds__(512)
+energy_kernel(const JrParams Pg, const int nmax, const float* positions,
+              const int32_t* types, const float* cell, const int32_t* n_atoms,
+              const float* pressure, const float* mu, double* energy64,
+              double* energy_u, float* forces, const int tpa) {
+  extern __shared__ __align__(16) unsigned char dyn[];
+  __shared__ WalkShared ws;
+  __shared__ JrParams P;
+  copy_params(P, Pg);
+  const int b = blockIdx.x;
+  const int n = n_atoms[b];
+  WalkArrays arr = carve(dyn, nmax, Pg.model.n_images);
+  Walker w{ws, arr, n, tpa, 0};
+  __syncthreads();
+  load_tables(P, ws);
+  for (int q = threadIdx.x; q < 3 * n; q += blockDim.x) {
+    pos_at(arr.xs, q) = positions[(size_t)b * nmax * 3 + q];
+    arr.dir[q] = 0.0f;
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    arr.xs[i].w = __int_as_float(types[(size_t)b * nmax + i]);
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < JR_MAX_SPECIES; ++q) ws.counts[q] = 0;
+    ws.cur = 0;
+    make_cell_ctx(cell + (size_t)b * 9, ws.cc[0], arr.T, P.model);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int i = 0; i < n; ++i) ws.counts[__float_as_int(arr.xs[i].w)] += 1;
+  __syncthreads();
+  double U, sff, sfd;
+  model_eval<true>(P, w, 0, U, sff, sfd);
+  const float* m = mu ? mu + (size_t)b * P.model.n_species : nullptr;
+  double E = U;
+  if (P.model.model != JR_MODEL_GAUSS_MIX)
+    E = U + ensemble_term(ws, ws.cc[0].vol, pressure[b], m, P.model.n_species);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    energy64[b] = E;
+    if (energy_u) energy_u[b] = U;
+  }
+  if (forces)
+    for (int q = threadIdx.x; q < 3 * n; q += blockDim.x)
+      forces[(size_t)b * nmax * 3 + q] = arr.F[q];
+}
+
+// --------------------------------------------------------- RE swaps ----
+__device__ double walker_ens(const JrDims& D, const JrStateBuffers& st, int p, int slot,
+                             int S) {
+  const int K = D.n_walkers, Nmax = D.n_atoms_max;
+  const size_t wb = (size_t)p * K + slot;
+  const float vol = fabsf(det3(st.cell + wb * 9));
+  double e = (double)st.pressure[p] * (double)vol;
+  if (st.mu) {
+    int counts[JR_MAX_SPECIES] = {0};
+    const int n = st.n_atoms[p];
+    for (int i = 0; i < n; ++i) counts[st.types[wb * Nmax + i]]++;
+    double dot = 0.0;
+    for (int q = 0; q < S; ++q) dot += (double)st.mu[(size_t)p * S + q] * (double)counts[q];
+    e = e - dot;
+  }
+  return e;
+}
+
+template <typename Tp>
+__device__ void swap_range(Tp* a, Tp* b, int n) {
+  for (int q = 0; q < n; ++q) {
+    Tp t = a[q];
+    a[q] = b[q];
+    b[q] = t;
+  }
+}
+
+// replica_exchange_step with EnsembleSwap (replica_exchange.py:318-436).
+__global__ void re_swap_kernel(const JrDims D, const JrStateBuffers st, const Key key,
+                               const int n_cycles, const int S, int* acc_pp,
+                               int* att_pp) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int R = D.n_replicas, K = D.n_walkers, Nmax = D.n_atoms_max;
+  const int n_even = R / 2, n_odd = (R - 1) / 2;
+  const int max_pairs = n_even > n_odd ? n_even : n_odd;
+  for (int q = 0; q < R - 1; ++q) {
+    if (acc_pp) acc_pp[q] = 0;
+    if (att_pp) att_pp[q] = 0;
+  }
+  for (int cyc = 0; cyc < n_cycles; ++cyc) {
+    const Key ck = split(key, (uint32_t)cyc);
+    for (int phase = 0; phase < 2; ++phase) {
+      const Key pk = split(ck, (uint32_t)phase);
+      const int nv = phase == 0 ? n_even : n_odd;
+      for (int slot = 0; slot < max_pairs; ++slot) {
+        const Key sk = split(pk, (uint32_t)slot);
+        const int wi = randint(split(sk, 0u), 0, K);
+        const int wj = randint(split(sk, 1u), 0, K);
+        if (slot >= nv) continue;
+        const int ri = phase + 2 * slot, rj = ri + 1;
+        const size_t bi = (size_t)ri * K + wi, bj = (size_t)rj * K + wj;
+        const double into_i = (st.energy64[bj] - walker_ens(D, st, rj, wj, S)) +
+                              [&] {
+                                // walker j's configuration in run i's ensemble
+                                const float vol = fabsf(det3(st.cell + bj * 9));
+                                double e = (double)st.pressure[ri] * (double)vol;
+                                if (st.mu) {
+                                  int cnt[JR_MAX_SPECIES] = {0};
+                                  for (int a = 0; a < st.n_atoms[rj]; ++a)
+                                    cnt[st.types[bj * Nmax + a]]++;
+                                  double dot = 0.0;
+                                  for (int q = 0; q < S; ++q)
+                                    dot += (double)st.mu[(size_t)ri * S + q] * (double)cnt[q];
+                                  e = e - dot;
+                                }
+                                return e;
+                              }();
+        const double into_j = (st.energy64[bi] - walker_ens(D, st, ri, wi, S)) +
+                              [&] {
+                                const float vol = fabsf(det3(st.cell + bi * 9));
+                                double e = (double)st.pressure[rj] * (double)vol;
+                                if (st.mu) {
+                                  int cnt[JR_MAX_SPECIES] = {0};
+                                  for (int a = 0; a < st.n_atoms[ri]; ++a)
+                                    cnt[st.types[bi * Nmax + a]]++;
+                                  double dot = 0.0;
+                                  for (int q = 0; q < S; ++q)
+                                    dot += (double)st.mu[(size_t)rj * S + q] * (double)cnt[q];
+                                  e = e - dot;
+                                }
+                                return e;
+                              }();
+        const bool do_swap = (into_i < st.emax[ri]) && (into_j < st.emax[rj]);
+        if (do_swap) {
+          swap_range(st.positions + bi * Nmax * 3, st.positions + bj * Nmax * 3, Nmax * 3);
+          swap_range(st.direction + bi * Nmax * 3, st.direction + bj * Nmax * 3, Nmax * 3);
+          swap_range(st.types + bi * Nmax, st.types + bj * Nmax, Nmax);
+          swap_range(st.cell + bi * 9, st.cell + bj * 9, 9);
+          st.energy64[bi] = into_i;
+          st.energy64[bj] = into_j;
+          st.energy[bi] = __double2float_rn(into_i);
+          st.energy[bj] = __double2float_rn(into_j);
+        }
+        if (acc_pp) acc_pp[ri] += do_swap ? 1 : 0;
+        if (att_pp) att_pp[ri] += 1;
+      }
+    }
+  }
+}
+
+}  // namespace jr
+
+// ================================================================ host ====
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+  return fail(JR_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+struct TuneKey {
+  int P, K, N, M, T, nx, S, nimg, model;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(P, K, N, M, T, nx, S, nimg, model) <
+           std::tie(o.P, o.K, o.N, o.M, o.T, o.nx, o.S, o.nimg, o.model);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, JrLaunchConfig> g_tune_cache;
+
+TuneKey tune_key(const JrDims* d, const JrParams* p) {
+  return TuneKey{d->n_replicas, d->n_walkers, d->n_atoms_max, d->n_moves,
+                 d->n_mcmc_steps, d->n_extra, p->model.n_species, p->model.n_images,
+                 p->model.model};
+}
+
+int pow2_floor(int x) {
+  int p = 1;
+  while (p * 2 <= x) p *= 2;
+  return p;
+}
+
+JrLaunchConfig heuristic_config(const JrDims* d) {
+  JrLaunchConfig c;
+  const int nmax = d->n_atoms_max;
+  c.threads = nmax <= 48 ? 256 : 512;
+  // as many threads per atom as the CTA allows, capped at 8
+  int tpa = pow2_floor(c.threads / (nmax > 0 ? nmax : 1));
+  if (tpa > 8) tpa = 8;
+  if (tpa < 1) tpa = 1;
+  c.tpa = tpa;
+  c.cluster = 1;
+  return c;
+}
+
+int check_params(const JrDims* d, const JrParams* p) {
+  if (!d || !p) return fail(JR_ERR_PARAM, "null dims or params");
+  if (d->n_replicas < 1 || d->n_walkers < 2 || d->n_atoms_max < 1 ||
+      d->n_atoms_max > JR_MAX_ATOMS)
+    return fail(JR_ERR_SHAPE, "need n_replicas>=1, n_walkers>=2, 1<=n_atoms_max<=" +
+                                  std::to_string(JR_MAX_ATOMS));
+  if (d->n_moves < 1 || d->n_moves > JR_MAX_MOVES || d->n_moves != p->moves.n_moves)
+    return fail(JR_ERR_SHAPE, "n_moves must be in [1, 8] and match params.moves");
+  if (d->n_cull != 1)
+    return fail(JR_ERR_UNSUPPORTED, "this build implements n_cull == 1 only");
+  if (d->n_extra < 0 || d->n_extra > d->n_walkers - 2 ||
+      d->n_extra + 1 > jr::kMaxWalk)
+    return fail(JR_ERR_SHAPE, "n_extra must satisfy 0 <= n_extra <= n_walkers-2 and <= 255");
+  if (p->model.n_species < 1 || p->model.n_species > JR_MAX_SPECIES)
+    return fail(JR_ERR_PARAM, "n_species must be in [1, 8]");
+  if (p->model.n_images < 1 || p->model.n_images > JR_MAX_IMAGES)
+    return fail(JR_ERR_PARAM, "n_images must be in [1, 125]");
+  for (int m = 0; m < d->n_moves; ++m) {
+    const int t = p->moves.type[m];
+    if (t < 0 || t > JR_MOVE_SWAP) return fail(JR_ERR_PARAM, "unknown move type");
+    if (t == JR_MOVE_GALILEAN && p->moves.n_reflect[m] < 1)
+      return fail(JR_ERR_PARAM, "galilean n_reflect must be >= 1");
+    if ((t == JR_MOVE_MORPH || t == JR_MOVE_SWAP) && p->model.n_species < 2)
+      return fail(JR_ERR_PARAM, "identity moves need n_species >= 2");
+  }
+  return JR_OK;
+}
+
+int check_config(const JrLaunchConfig& c, const JrDims* d) {
+  if (c.threads < 32 || c.threads > 512 || (c.threads & 31))
+    return fail(JR_ERR_PARAM, "threads must be a multiple of 32 in [32, 512]");
+  if (c.tpa < 1 || c.tpa > 32 || (c.tpa & (c.tpa - 1)))
+    return fail(JR_ERR_PARAM, "tpa must be a power of two <= 32");
+  if (c.cluster < 1 || c.cluster > 16)
+    return fail(JR_ERR_PARAM, "cluster must be in [1, 16]");
+  const int W = 1 + d->n_extra;
+  if (c.cluster >= 2 * W && (c.cluster / W) * d->n_extra > jr::kMaxWalk)
+    return fail(JR_ERR_PARAM, "cluster * n_extra too large for speculation");
+  return JR_OK;
+}
+
+size_t ns_dyn_smem(const JrDims* d, const JrParams* p) {
+  return jr::walk_dyn_smem_bytes(d->n_atoms_max, p->model.n_images) +
+         (size_t)d->n_walkers * (sizeof(double) + sizeof(float));
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* jr_last_error(void) { return g_last_error.c_str(); }
+
+int jr_version(void) { return 1; }
+
+size_t jr_ns_iterate_workspace_size(const JrDims* dims) {
+  (void)dims;
+  return 256;
+}
+
+int jr_ns_iterate(const JrDims* dims, const JrParams* params,
+                  const JrStateBuffers* state, const JrInfoBuffers* info,
+                  int32_t n_iter, const JrLaunchConfig* cfg, void* workspace,
+                  size_t workspace_bytes, void* stream) {
+  int rc = check_params(dims, params);
+  if (rc) return rc;
+  if (!state) return fail(JR_ERR_PARAM, "null state");
+  if (n_iter < 1) return fail(JR_ERR_PARAM, "n_iter must be >= 1");
+  if (!workspace || workspace_bytes < jr_ns_iterate_workspace_size(dims))
+    return fail(JR_ERR_WORKSPACE, "workspace missing or smaller than jr_ns_iterate_workspace_size()");
+  JrLaunchConfig c;
+  if (cfg) {
+    c = *cfg;
+  } else {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(tune_key(dims, params));
+    c = it != g_tune_cache.end() ? it->second : heuristic_config(dims);
+  }
+  rc = check_config(c, dims);
+  if (rc) return rc;
+  JrInfoBuffers inf{};
+  if (info) inf = *info;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(workspace, state->rng_key, 2 * sizeof(uint32_t),
+                                  cudaMemcpyDeviceToDevice, s);
+  if (e != cudaSuccess) return cuda_fail(e, "key snapshot");
+  const size_t smem = ns_dyn_smem(dims, params);
+  e = cudaFuncSetAttribute(jr::ns_iterate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+  if (e != cudaSuccess) return cuda_fail(e, "smem attribute");
+  if (c.cluster > 8) {
+    e = cudaFuncSetAttribute(jr::ns_iterate_kernel,
+                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return cuda_fail(e, "non-portable cluster attribute");
+  }
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(dims->n_replicas * c.cluster);
+  lc.blockDim = dim3(c.threads);
+  lc.dynamicSmemBytes = smem;
+  lc.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = c.cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  lc.attrs = attr;
+  lc.numAttrs = 1;
+  e = cudaLaunchKernelEx(&lc, jr::ns_iterate_kernel, *dims, *params, *state, inf,
+                         (int)n_iter, (int)c.tpa, (int)c.cluster,
+                         (const uint32_t*)workspace);
+  if (e != cudaSuccess) return cuda_fail(e, "ns_iterate launch");
+  return JR_OK;
+}
+
+int jr_move_trial(const JrDims* dims, const JrParams* params,
+                  const JrStateBuffers* state, int32_t n_trials, int32_t move_idx,
+                  const int32_t* walker_idx, const uint32_t* keys,
+                  const uint32_t* move_keys, const float* step, const double* emax,
+                  int32_t write_back, int32_t* accepted, int32_t* reject_reason,
+                  void* stream) {
+  int rc = check_params(dims, params);
+  if (rc) return rc;
+  if (n_trials < 1 || !walker_idx || !keys || !step || !emax || !accepted)
+    return fail(JR_ERR_PARAM, "trial buffers missing or n_trials < 1");
+  if (move_idx >= dims->n_moves) return fail(JR_ERR_PARAM, "move_idx out of range");
+  if (move_idx < 0 && !move_keys) return fail(JR_ERR_PARAM, "move_keys needed when move_idx < 0");
+  JrLaunchConfig c = heuristic_config(dims);
+  const size_t smem = jr::walk_dyn_smem_bytes(dims->n_atoms_max, params->model.n_images);
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaFuncSetAttribute(jr::move_trial_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return cuda_fail(e, "smem attribute");
+  jr::move_trial_kernel<<<dims->n_replicas * n_trials, c.threads, smem, s>>>(
+      *dims, *params, *state, n_trials, move_idx, walker_idx, keys, move_keys, step, emax,
+      write_back, accepted, reject_reason, c.tpa);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "move_trial launch");
+  return JR_OK;
+}
+
+int jr_energy_forces(const JrParams* params, int32_t n_configs, int32_t n_atoms_max,
+                     const float* positions, const int32_t* types, const float* cell,
+                     const int32_t* n_atoms, const float* pressure, const float* mu,
+                     double* energy64, double* energy_u, float* forces, void* stream) {
+  if (!params || n_configs < 1 || n_atoms_max < 1 || n_atoms_max > JR_MAX_ATOMS ||
+      !positions || !types || !cell || !n_atoms || !pressure || !energy64)
+    return fail(JR_ERR_PARAM, "invalid energy_forces arguments");
+  if (params->model.n_species < 1 || params->model.n_species > JR_MAX_SPECIES ||
+      params->model.n_images < 1 || params->model.n_images > JR_MAX_IMAGES)
+    return fail(JR_ERR_PARAM, "invalid model parameters");
+  JrDims d{};
+  d.n_atoms_max = n_atoms_max;
+  JrLaunchConfig c = heuristic_config(&d);
+  const size_t smem = jr::walk_dyn_smem_bytes(n_atoms_max, params->model.n_images);
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaFuncSetAttribute(jr::energy_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return cuda_fail(e, "smem attribute");
+  jr::energy_kernel<<<n_configs, c.threads, smem, s>>>(*params, n_atoms_max, positions, types,
+                                                      cell, n_atoms, pressure, mu, energy64,
+                                                      energy_u, forces, c.tpa);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "energy launch");
+  return JR_OK;
+}
+
+int jr_re_swap(const JrDims* dims, const JrStateBuffers* state, uint32_t key0,
+               uint32_t key1, int32_t n_swap_cycles, int32_t n_species,
+               int32_t* acc_per_pair, int32_t* att_per_pair, void* stream) {
+  if (!dims || !state) return fail(JR_ERR_PARAM, "null dims or state");
+  if (n_swap_cycles < 0 || n_species < 1 || n_species > JR_MAX_SPECIES)
+    return fail(JR_ERR_PARAM, "invalid swap parameters");
+  if (dims->n_replicas < 2) return JR_OK;
+  jr::re_swap_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(
+      *dims, *state, jr::Key{key0, key1}, n_swap_cycles, n_species, acc_per_pair,
+      att_per_pair);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "re_swap launch");
+  return JR_OK;
+}
+
+}  // extern "C"
+
+// ============================================================ autotune ====
+namespace {
+
+struct ScratchState {
+  JrStateBuffers b{};
+  void* blocks[16] = {};
+  int nblk = 0;
+  ~ScratchState() {
+    for (int i = 0; i < nblk; ++i) cudaFree(blocks[i]);
+  }
+  void* take(size_t bytes) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    blocks[nblk++] = p;
+    return p;
+  }
+};
+
+// Scratch copy of the mutable state so candidate launch shapes can be timed
+// without touching the caller's walkers.  Freed before jr_autotune returns.
+int clone_state(const JrDims* d, const JrParams* p, const JrStateBuffers* s,
+                ScratchState& out, cudaStream_t st) {
+  const size_t PK = (size_t)d->n_replicas * d->n_walkers;
+  const size_t N = d->n_atoms_max, M = d->n_moves;
+  struct F {
+    const void* src;
+    size_t bytes;
+    void** dst;
+  };
+  out.b = *s;
+  F fields[] = {
+      {s->positions, PK * N * 3 * 4, (void**)&out.b.positions},
+      {s->direction, PK * N * 3 * 4, (void**)&out.b.direction},
+      {s->types, PK * N * 4, (void**)&out.b.types},
+      {s->energy, PK * 4, (void**)&out.b.energy},
+      {s->energy64, PK * 8, (void**)&out.b.energy64},
+      {s->cell, PK * 9 * 4, (void**)&out.b.cell},
+      {s->step_sizes, PK * M * 4, (void**)&out.b.step_sizes},
+      {s->n_accepted, PK * M * 4, (void**)&out.b.n_accepted},
+      {s->n_proposed, PK * M * 4, (void**)&out.b.n_proposed},
+      {s->rng_key, (size_t)d->n_replicas * 8, (void**)&out.b.rng_key},
+      {s->log_evidence, (size_t)d->n_replicas * 8, (void**)&out.b.log_evidence},
+      {s->iteration, (size_t)d->n_replicas * 4, (void**)&out.b.iteration},
+      {s->emax, (size_t)d->n_replicas * 8, (void**)&out.b.emax},
+  };
+  (void)p;
+  for (auto& f : fields) {
+    void* q = out.take(f.bytes);
+    if (!q) return fail(JR_ERR_CUDA, "autotune scratch allocation failed");
+    cudaError_t e = cudaMemcpyAsync(q, f.src, f.bytes, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(e, "autotune scratch copy");
+    *f.dst = q;
+  }
+  return JR_OK;
+}
+
+}  // namespace
+
+extern "C" int jr_autotune(const JrDims* dims, const JrParams* params,
+                           const JrStateBuffers* state, int32_t n_iter_probe,
+                           JrLaunchConfig* best, void* stream) {
+  int rc = check_params(dims, params);
+  if (rc) return rc;
+  if (!state || !best || n_iter_probe < 1) return fail(JR_ERR_PARAM, "autotune arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  ScratchState scratch;
+  rc = clone_state(dims, params, state, scratch, st);
+  if (rc) return rc;
+  void* ws = scratch.take(jr_ns_iterate_workspace_size(dims));
+  if (!ws) return fail(JR_ERR_CUDA, "autotune workspace allocation failed");
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int W = 1 + dims->n_extra;
+  float best_ms = 1e30f;
+  JrLaunchConfig bc = heuristic_config(dims);
+  const int thread_opts[] = {128, 256, 512};
+  const int tpa_opts[] = {2, 4, 8, 16, 32};
+  const int cluster_opts[] = {1, 2, 4, 8, 10, 12, 16};
+  for (int th : thread_opts) {
+    if (th / 32 > jr::kMaxWarps) continue;
+    for (int tpa : tpa_opts) {
+      if (tpa > th) continue;
+      // keep at least one pass worth of atoms busy
+      if (th / tpa > 4 * dims->n_atoms_max && tpa < 32) continue;
+      for (int cl : cluster_opts) {
+        if (cl > 1 && cl < 2 * W && cl != W) continue;
+        JrLaunchConfig c{th, tpa, cl};
+        if (check_config(c, dims) != JR_OK) continue;
+        // warm-up launch (also rejects shapes the hardware cannot place)
+        rc = jr_ns_iterate(dims, params, &scratch.b, nullptr, 1, &c, ws, 256, stream);
+        if (rc != JR_OK || cudaStreamSynchronize(st) != cudaSuccess) {
+          cudaGetLastError();
+          continue;
+        }
+        cudaEventRecord(e0, st);
+        rc = jr_ns_iterate(dims, params, &scratch.b, nullptr, n_iter_probe, &c, ws, 256, stream);
+        cudaEventRecord(e1, st);
+        if (rc != JR_OK || cudaEventSynchronize(e1) != cudaSuccess) {
+          cudaGetLastError();
+          continue;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+          best_ms = ms;
+          bc = c;
+        }
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamSynchronize(st);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[tune_key(dims, params)] = bc;
+  }
+  *best = bc;
+  g_last_error.clear();
+  return JR_OK;
+}
+
+// ======================================================= measurement ====
+namespace jr {
+// Independent FMA chains per thread: the FP32 FMA pipe's attainable rate.
+__global__ void __launch_bounds__(256) fma_peak_kernel(float* out, int iters) {
+  float a0 = threadIdx.x * 1e-7f, a1 = a0 + 1e-7f, a2 = a0 + 2e-7f, a3 = a0 + 3e-7f;
+  float a4 = a0 + 4e-7f, a5 = a0 + 5e-7f, a6 = a0 + 6e-7f, a7 = a0 + 7e-7f;
+  const float b = 0.999999f, c = 1e-7f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      a0 = __fmaf_rn(a0, b, c); a1 = __fmaf_rn(a1, b, c);
+      a2 = __fmaf_rn(a2, b, c); a3 = __fmaf_rn(a3, b, c);
+      a4 = __fmaf_rn(a4, b, c); a5 = __fmaf_rn(a5, b, c);
+      a6 = __fmaf_rn(a6, b, c); a7 = __fmaf_rn(a7, b, c);
+    }
+  }
+  const float s = ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
+  if (s == 12345.678f) out[blockIdx.x] = s;  // keeps the chains live
+}
+}  // namespace jr
+
+extern "C" int jr_bench_fma_peak(int n_blocks, int iters, float* scratch, double* flops,
+                                 void* stream) {
+  if (n_blocks < 1 || iters < 1 || !scratch || !flops)
+    return fail(JR_ERR_PARAM, "fma_peak arguments");
+  jr::fma_peak_kernel<<<n_blocks, 256, 0, (cudaStream_t)stream>>>(scratch, iters);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "fma_peak launch");
+  *flops = 2.0 * 8.0 * 16.0 * (double)iters * 256.0 * (double)n_blocks;
+  return JR_OK;
+}

@@ -1,0 +1,831 @@
+// jr_walk.cuh -- one walker resident in shared memory, walked by a whole CTA.
+//
+// Arithmetic contract (shared with the CPU oracle's DEV mode):
+//   * pair terms in float32 with a fixed FMA placement (explicit intrinsics,
+//     the translation unit is compiled with -fmad=false),
+//   * every sum (energy, forces, norms, dot products) accumulated in float64
+//     and rounded to float32 once where a float32 value is needed.
+// Because the float64 sums of float32 terms are exact for any configuration
+// whose pair terms span < 2^29 in magnitude, results do not depend on the
+// thread mapping (launch shape) and match the oracle bit-for-bit.
+#pragma once
+#include <cstdint>
+
+#include "../../include/jaxrens_b200.h"
+#include "jr_rng.cuh"
+
+namespace jr {
+
+constexpr int kMaxWarps = 32;
+
+// Geometry of one cell: the matrix, its inverse and the image translations.
+struct CellCtx {
+  float raw[9];  // the cell as stored (rows are lattice vectors)
+  float h[9];    // the cell used for geometry (1e10*I when det == 0)
+  float inv[9];
+  int diag;
+  float vol;  // |det(h)| of the un-substituted cell (ensemble term)
+};
+
+// Fixed-size per-CTA state; the per-atom arrays live in dynamic smem.
+struct WalkShared {
+  CellCtx cc[2];        // [cur], [trial]
+  int cur;              // index of the current cell context
+  double E;             // current full potential of the walker
+  float step_sizes[JR_MAX_MOVES];
+  int counts[JR_MAX_SPECIES];
+  float sig2[JR_MAX_SPECIES * JR_MAX_SPECIES];
+  float eps4[JR_MAX_SPECIES * JR_MAX_SPECIES];
+  float eps24[JR_MAX_SPECIES * JR_MAX_SPECIES];
+  // per-walker MWG counters (MCState.n_accepted / n_proposed)
+  int w_acc[JR_MAX_MOVES];
+  int w_prop[JR_MAX_MOVES];
+  // per-chain info counters (ns_step info dict), summed over steps
+  int c_acc[JR_MAX_MOVES];
+  int c_prop[JR_MAX_MOVES];
+  int c_rr[JR_MAX_MOVES * 4];
+  int c_nev[JR_MAX_MOVES];
+  int c_ngr[JR_MAX_MOVES];
+  double red[2][kMaxWarps][3];
+  int bcast_i[4];
+  float bcast_f[4];
+};
+
+// Dynamic shared memory carve-up for Nmax atoms and n_img images.
+struct WalkArrays {
+  float4* xs;   // [Nmax] position + type bits (current / trial positions)
+  float* x0;    // [3 Nmax] saved positions
+  float* dir;   // [3 Nmax] direction
+  float* dp;    // [3 Nmax] perturbed direction (flip target on reject)
+  float* F;     // [3 Nmax] forces
+  float* T;     // [2][3 n_img] image translations for cc[0], cc[1]
+};
+
+__host__ __device__ inline size_t walk_dyn_smem_bytes(int nmax, int nimg) {
+  size_t b = 16u * (size_t)nmax + 4u * 12u * (size_t)nmax + 2u * 3u * 4u * (size_t)nimg;
+  return (b + 15) & ~(size_t)15;
+}
+
+__device__ inline WalkArrays carve(void* dyn, int nmax, int nimg) {
+  WalkArrays a;
+  char* p = (char*)dyn;
+  a.xs = (float4*)p; p += 16 * nmax;
+  a.x0 = (float*)p; p += 12 * nmax;
+  a.dir = (float*)p; p += 12 * nmax;
+  a.dp = (float*)p; p += 12 * nmax;
+  a.F = (float*)p; p += 12 * nmax;
+  a.T = (float*)p;
+  return a;
+}
+
+// Per-thread view of the walker: the shared state, the smem arrays, the atom
+// count, the pair-loop mapping and this thread's copy of the reduction-buffer
+// parity (block-uniform, flipped by every block reduction).
+struct Walker {
+  WalkShared& s;
+  WalkArrays arr;
+  int n;
+  int tpa;
+  int par;
+};
+
+__device__ __forceinline__ float& pos_at(float4* xs, int idx) {
+  return reinterpret_cast<float*>(xs)[4 * (idx / 3) + (idx % 3)];
+}
+
+// jnp.linalg.det of a 3x3 (jax _det_3x3), float32, left to right.
+__device__ __forceinline__ float det3(const float* a) {
+  float t1 = __fmul_rn(__fmul_rn(a[0], a[4]), a[8]);
+  float t2 = __fmul_rn(__fmul_rn(a[1], a[5]), a[6]);
+  float t3 = __fmul_rn(__fmul_rn(a[2], a[3]), a[7]);
+  float t4 = __fmul_rn(__fmul_rn(a[2], a[4]), a[6]);
+  float t5 = __fmul_rn(__fmul_rn(a[0], a[5]), a[7]);
+  float t6 = __fmul_rn(__fmul_rn(a[1], a[3]), a[8]);
+  float s = __fadd_rn(t1, t2);
+  s = __fadd_rn(s, t3);
+  s = __fsub_rn(s, t4);
+  s = __fsub_rn(s, t5);
+  s = __fsub_rn(s, t6);
+  return s;
+}
+
+// Fill a cell context: det==0 substitutes 1e10*I (lj.py:136-137); a diagonal
+// cell inverts with float32 division, any other through the double adjugate.
+__device__ inline void make_cell_ctx(const float* h_in, CellCtx& cc,
+                                     float* T, const JrModelParams& mp) {
+  cc.vol = fabsf(det3(h_in));
+  for (int q = 0; q < 9; ++q) cc.raw[q] = h_in[q];
+  float h[9];
+  if (det3(h_in) == 0.0f) {
+    for (int q = 0; q < 9; ++q) h[q] = 0.0f;
+    h[0] = h[4] = h[8] = 1.0e10f;
+  } else {
+    for (int q = 0; q < 9; ++q) h[q] = h_in[q];
+  }
+  for (int q = 0; q < 9; ++q) cc.h[q] = h[q];
+  const bool diag = h[1] == 0.0f && h[2] == 0.0f && h[3] == 0.0f &&
+                    h[5] == 0.0f && h[6] == 0.0f && h[7] == 0.0f;
+  cc.diag = diag;
+  if (diag) {
+    for (int q = 0; q < 9; ++q) cc.inv[q] = 0.0f;
+    cc.inv[0] = __fdiv_rn(1.0f, h[0]);
+    cc.inv[4] = __fdiv_rn(1.0f, h[4]);
+    cc.inv[8] = __fdiv_rn(1.0f, h[8]);
+  } else {
+    double a[9], cof[9];
+    for (int q = 0; q < 9; ++q) a[q] = (double)h[q];
+    cof[0] = __dsub_rn(__dmul_rn(a[4], a[8]), __dmul_rn(a[5], a[7]));
+    cof[1] = __dsub_rn(__dmul_rn(a[5], a[6]), __dmul_rn(a[3], a[8]));
+    cof[2] = __dsub_rn(__dmul_rn(a[3], a[7]), __dmul_rn(a[4], a[6]));
+    cof[3] = __dsub_rn(__dmul_rn(a[2], a[7]), __dmul_rn(a[1], a[8]));
+    cof[4] = __dsub_rn(__dmul_rn(a[0], a[8]), __dmul_rn(a[2], a[6]));
+    cof[5] = __dsub_rn(__dmul_rn(a[1], a[6]), __dmul_rn(a[0], a[7]));
+    cof[6] = __dsub_rn(__dmul_rn(a[1], a[5]), __dmul_rn(a[2], a[4]));
+    cof[7] = __dsub_rn(__dmul_rn(a[2], a[3]), __dmul_rn(a[0], a[5]));
+    cof[8] = __dsub_rn(__dmul_rn(a[0], a[4]), __dmul_rn(a[1], a[3]));
+    double det = __dadd_rn(__dadd_rn(__dmul_rn(a[0], cof[0]), __dmul_rn(a[1], cof[1])),
+                           __dmul_rn(a[2], cof[2]));
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        cc.inv[i * 3 + j] = __double2float_rn(__ddiv_rn(cof[j * 3 + i], det));
+  }
+  for (int k = 0; k < mp.n_images; ++k) {
+    const float* o = mp.img_off + 3 * k;
+    for (int q = 0; q < 3; ++q) {
+      float v = __fmul_rn(o[0], h[q]);
+      v = __fmaf_rn(o[1], h[3 + q], v);
+      v = __fmaf_rn(o[2], h[6 + q], v);
+      T[3 * k + q] = v;
+    }
+  }
+}
+
+// Triclinic minimum image: dr - round(dr @ inv) @ h (lj.py:147-154).
+__device__ __forceinline__ void mic(const CellCtx& cc, float& dx, float& dy,
+                                    float& dz) {
+  if (cc.diag) {
+    float n0 = rintf(__fmul_rn(dx, cc.inv[0]));
+    float n1 = rintf(__fmul_rn(dy, cc.inv[4]));
+    float n2 = rintf(__fmul_rn(dz, cc.inv[8]));
+    dx = __fsub_rn(dx, __fmul_rn(n0, cc.h[0]));
+    dy = __fsub_rn(dy, __fmul_rn(n1, cc.h[4]));
+    dz = __fsub_rn(dz, __fmul_rn(n2, cc.h[8]));
+  } else {
+    float n[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      float f = __fmul_rn(dx, cc.inv[q]);
+      f = __fmaf_rn(dy, cc.inv[3 + q], f);
+      f = __fmaf_rn(dz, cc.inv[6 + q], f);
+      n[q] = rintf(f);
+    }
+    float s[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      float v = __fmul_rn(n[0], cc.h[q]);
+      v = __fmaf_rn(n[1], cc.h[3 + q], v);
+      v = __fmaf_rn(n[2], cc.h[6 + q], v);
+      s[q] = v;
+    }
+    dx = __fsub_rn(dx, s[0]);
+    dy = __fsub_rn(dy, s[1]);
+    dz = __fsub_rn(dz, s[2]);
+  }
+}
+
+// One LJ pair term (lj.py:191-203), float32: energy e and the force
+// coefficient g with F_i += g * dr_ij.
+__device__ __forceinline__ void lj_pair(float dx, float dy, float dz,
+                                        float sig2, float eps4, float eps24,
+                                        bool has_cut, float rc2, float& e,
+                                        float& g) {
+  float r2 = __fmul_rn(dx, dx);
+  r2 = __fmaf_rn(dy, dy, r2);
+  r2 = __fmaf_rn(dz, dz, r2);
+  if (has_cut && !(r2 < rc2)) {
+    e = 0.0f;
+    g = 0.0f;
+    return;
+  }
+  float ri = __frcp_rn(r2);
+  float s2 = __fmul_rn(sig2, ri);
+  float s4 = __fmul_rn(s2, s2);
+  float s6 = __fmul_rn(s4, s2);
+  float s12 = __fmul_rn(s6, s6);
+  e = __fmul_rn(eps4, __fsub_rn(s12, s6));
+  float t = __fmaf_rn(2.0f, s12, -s6);
+  float a = __fmul_rn(eps24, ri);
+  g = -__fmul_rn(a, t);
+}
+
+// Block-wide sum of three doubles; lanes hold partials only at multiples of
+// `lane_stride` (a power of two).  Deterministic: warps summed in order.  The
+// two partial buffers alternate, so one barrier per reduction suffices.
+__device__ __forceinline__ void block_sum3(Walker& w, double& a, double& b,
+                                           double& c, int lane_stride) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+  for (int off = 16; off >= lane_stride; off >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, off);
+    b += __shfl_xor_sync(0xffffffffu, b, off);
+    c += __shfl_xor_sync(0xffffffffu, c, off);
+  }
+  double (*buf)[3] = w.s.red[w.par];
+  if (lane == 0) {
+    buf[warp][0] = a;
+    buf[warp][1] = b;
+    buf[warp][2] = c;
+  }
+  __syncthreads();
+  a = 0.0; b = 0.0; c = 0.0;
+  for (int q = 0; q < nw; ++q) {
+    a += buf[q][0];
+    b += buf[q][1];
+    c += buf[q][2];
+  }
+  w.par ^= 1;
+}
+
+// Ensemble term P*V - mu*N (ensemble.py:34-59) in float64.
+__device__ __forceinline__ double ensemble_term(const WalkShared& s, float vol,
+                                                float pressure, const float* mu,
+                                                int nsp) {
+  double e = (double)pressure * (double)vol;
+  if (mu) {
+    double dot = 0.0;
+    for (int q = 0; q < nsp; ++q) dot += (double)mu[q] * (double)s.counts[q];
+    e = e - dot;
+  }
+  return e;
+}
+
+// Gaussian-mixture toy (toy.py:163-204), float64, forces rounded to float32.
+__device__ inline double gauss_mix_energy(const JrModelParams& mp, const float4* xs,
+                                          int n, float* F, bool forces) {
+  double com[3] = {0, 0, 0};
+  for (int i = 0; i < n; ++i) {
+    com[0] += (double)xs[i].x;
+    com[1] += (double)xs[i].y;
+    com[2] += (double)xs[i].z;
+  }
+  for (int q = 0; q < 3; ++q) com[q] /= (double)n;
+  const double s2 = (double)mp.gm_sigma * (double)mp.gm_sigma;
+  const double lnorm = 1.5 * log(2.0 * 3.141592653589793 * s2);
+  double l[JR_MAX_CENTERS], lmax = -INFINITY;
+  for (int k = 0; k < mp.n_centers; ++k) {
+    double ds = 0.0;
+    for (int q = 0; q < 3; ++q) {
+      double df = com[q] - (double)mp.centers[3 * k + q];
+      ds += df * df;
+    }
+    l[k] = -0.5 * ds / s2 - lnorm;
+    if (l[k] > lmax) lmax = l[k];
+  }
+  double z = 0.0;
+  for (int k = 0; k < mp.n_centers; ++k) z += exp(l[k] - lmax);
+  const double E = -(lmax + log(z));
+  if (forces) {
+    double g[3] = {0, 0, 0};
+    for (int k = 0; k < mp.n_centers; ++k) {
+      double p = exp(l[k] - lmax) / z;
+      for (int q = 0; q < 3; ++q) g[q] += p * (com[q] - (double)mp.centers[3 * k + q]) / s2;
+    }
+    for (int i = 0; i < n; ++i)
+      for (int q = 0; q < 3; ++q) F[3 * i + q] = (float)(-g[q] / (double)n);
+  }
+  return E;
+}
+
+__device__ __forceinline__ int center_image(const JrModelParams& mp) {
+  for (int k = 0; k < mp.n_images; ++k)
+    if (mp.img_off[3 * k] == 0.0f && mp.img_off[3 * k + 1] == 0.0f &&
+        mp.img_off[3 * k + 2] == 0.0f)
+      return k;
+  return -1;
+}
+
+// Model energy U (forces into arr.F when kForces) of the walker in smem; also
+// returns sum(F^2) and sum(F . dir) for the galilean reflection.  All threads
+// call it; the results are block-uniform on return.
+template <bool kForces>
+__device__ void model_eval(const JrParams& P, Walker& w, int cidx, double& U,
+                           double& sff, double& sfd) {
+  WalkShared& s = w.s;
+  const WalkArrays& arr = w.arr;
+  const int n = w.n, tpa = w.tpa;
+  const JrModelParams& mp = P.model;
+  if (mp.model == JR_MODEL_GAUSS_MIX) {
+    double e = 0.0, a = 0.0, b = 0.0;
+    if (threadIdx.x == 0) {
+      e = gauss_mix_energy(mp, arr.xs, n, arr.F, kForces);
+      if (kForces) {
+        for (int q = 0; q < 3 * n; ++q) {
+          a += (double)arr.F[q] * (double)arr.F[q];
+          b += (double)arr.F[q] * (double)arr.dir[q];
+        }
+      }
+    }
+    block_sum3(w, e, a, b, 1);
+    U = e;
+    sff = a;
+    sfd = b;
+    return;
+  }
+  const CellCtx& cc = s.cc[cidx];
+  const float* T = arr.T + cidx * 3 * mp.n_images;
+  const int nimg = mp.n_images;
+  const bool has_cut = mp.has_cutoff != 0;
+  const float rc2 = mp.rc2;
+  const int nsp = mp.n_species;
+  const int tid = threadIdx.x;
+  const int apb = blockDim.x / tpa;
+  const int g0 = tid % tpa;
+  const int center = center_image(mp);
+  double e_part = 0.0, ff_part = 0.0, fd_part = 0.0;
+  for (int base = 0; base < n; base += apb) {
+    const int i = base + tid / tpa;
+    double fx = 0.0, fy = 0.0, fz = 0.0, ei = 0.0;
+    if (i < n) {
+      const float4 xi = arr.xs[i];
+      const int ti = __float_as_int(xi.w);
+      for (int j = g0; j < n; j += tpa) {
+        const float4 xj = arr.xs[j];
+        const int tj = __float_as_int(xj.w);
+        float dx = __fsub_rn(xj.x, xi.x);
+        float dy = __fsub_rn(xj.y, xi.y);
+        float dz = __fsub_rn(xj.z, xi.z);
+        mic(cc, dx, dy, dz);
+        const int pt = ti * nsp + tj;
+        const float sig2 = s.sig2[pt], eps4 = s.eps4[pt], eps24 = s.eps24[pt];
+        if (nimg == 1) {
+          if (j != i) {
+            float e, g;
+            lj_pair(dx, dy, dz, sig2, eps4, eps24, has_cut, rc2, e, g);
+            ei += (double)e;
+            if (kForces) {
+              fx += (double)__fmul_rn(g, dx);
+              fy += (double)__fmul_rn(g, dy);
+              fz += (double)__fmul_rn(g, dz);
+            }
+          }
+        } else {
+          for (int k = 0; k < nimg; ++k) {
+            if (k == center && i == j) continue;
+            const float ex = __fadd_rn(dx, T[3 * k]);
+            const float ey = __fadd_rn(dy, T[3 * k + 1]);
+            const float ez = __fadd_rn(dz, T[3 * k + 2]);
+            float e, g;
+            lj_pair(ex, ey, ez, sig2, eps4, eps24, has_cut, rc2, e, g);
+            ei += (double)e;
+            if (kForces && i != j) {
+              fx += (double)__fmul_rn(g, ex);
+              fy += (double)__fmul_rn(g, ey);
+              fz += (double)__fmul_rn(g, ez);
+            }
+          }
+        }
+      }
+    }
+    for (int off = tpa >> 1; off > 0; off >>= 1) {
+      ei += __shfl_xor_sync(0xffffffffu, ei, off);
+      if (kForces) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, off);
+        fy += __shfl_xor_sync(0xffffffffu, fy, off);
+        fz += __shfl_xor_sync(0xffffffffu, fz, off);
+      }
+    }
+    if (g0 == 0 && i < n) {
+      e_part += ei;
+      if (kForces) {
+        const float Fx = __double2float_rn(fx), Fy = __double2float_rn(fy),
+                    Fz = __double2float_rn(fz);
+        arr.F[3 * i] = Fx;
+        arr.F[3 * i + 1] = Fy;
+        arr.F[3 * i + 2] = Fz;
+        ff_part += (double)Fx * (double)Fx + (double)Fy * (double)Fy +
+                   (double)Fz * (double)Fz;
+        fd_part += (double)Fx * (double)arr.dir[3 * i] +
+                   (double)Fy * (double)arr.dir[3 * i + 1] +
+                   (double)Fz * (double)arr.dir[3 * i + 2];
+      }
+    }
+  }
+  block_sum3(w, e_part, ff_part, fd_part, tpa);
+  U = 0.5 * e_part;
+  sff = ff_part;
+  sfd = fd_part;
+}
+
+// Full potential of the walker for cell context cidx: U + (P*V - mu*N).
+template <bool kForces>
+__device__ __forceinline__ double ham_eval(const JrParams& P, Walker& w, int cidx,
+                                           float pressure, const float* mu,
+                                           double& sff, double& sfd) {
+  double U;
+  model_eval<kForces>(P, w, cidx, U, sff, sfd);
+  if (P.model.model == JR_MODEL_GAUSS_MIX) return U;
+  return U + ensemble_term(w.s, w.s.cc[cidx].vol, pressure, mu, P.model.n_species);
+}
+
+__device__ __forceinline__ double block_sum1(Walker& w, double v) {
+  double b = 0.0, c = 0.0;
+  block_sum3(w, v, b, c, 1);
+  return v;
+}
+
+// ---------------------------------------------------------------- moves --
+
+// Galilean move (galilean.py:142-300) with forces-based reflection.  The
+// reflection d - 2 (f.d) f with f = F/|F| is evaluated as
+// d - [2 (F.d) / max(|F|,1e-10)^2] F from two float64 sums.
+__device__ bool move_galilean(const JrParams& P, Walker& w, Key key, float step,
+                              int R, float pa, double emax, float pressure,
+                              const float* mu) {
+  const WalkArrays& arr = w.arr;
+  const int n3 = 3 * w.n;
+  const Key ki = split(key, 0u), kp = split(key, 1u);
+  double sq = 0.0;
+  for (int q = threadIdx.x; q < n3; q += blockDim.x)
+    sq += (double)arr.dir[q] * (double)arr.dir[q];
+  sq = block_sum1(w, sq);
+  const bool fresh = __double2float_rn(sqrt(sq)) < 1e-8f;
+  double sv = 0.0;
+  for (int q = threadIdx.x; q < n3; q += blockDim.x) {
+    float v;
+    if (fresh) {
+      v = normal(bits32(ki, (uint32_t)q));
+    } else {
+      v = __fmaf_rn(pa, normal(bits32(kp, (uint32_t)q)), arr.dir[q]);
+    }
+    arr.dir[q] = v;
+    sv += (double)v * (double)v;
+  }
+  sv = block_sum1(w, sv);
+  const float nv = __double2float_rn(sqrt(sv));
+  const float den = nv > 1e-10f ? nv : 1e-10f;
+  for (int q = threadIdx.x; q < n3; q += blockDim.x) {
+    const float v = __fdiv_rn(arr.dir[q], den);
+    arr.dir[q] = v;
+    arr.dp[q] = v;
+    arr.x0[q] = pos_at(arr.xs, q);
+  }
+  const double E0 = w.s.E;
+  double E = E0;
+  for (int r = 0; r < R; ++r) {
+    for (int q = threadIdx.x; q < n3; q += blockDim.x) {
+      float& x = pos_at(arr.xs, q);
+      x = __fmaf_rn(step, arr.dir[q], x);
+    }
+    __syncthreads();
+    double sff, sfd;
+    E = ham_eval<true>(P, w, w.s.cur, pressure, mu, sff, sfd);
+    if (isnan(E)) E = INFINITY;
+    if (E >= emax) {
+      double nrm = sqrt(sff);
+      if (nrm < 1e-10) nrm = 1e-10;
+      const float coef = __double2float_rn(__ddiv_rn(2.0 * sfd, nrm * nrm));
+      for (int q = threadIdx.x; q < n3; q += blockDim.x)
+        arr.dir[q] = __fmaf_rn(-coef, arr.F[q], arr.dir[q]);
+    }
+  }
+  const bool acc = E < emax;
+  if (!acc) {
+    for (int q = threadIdx.x; q < n3; q += blockDim.x) {
+      pos_at(arr.xs, q) = arr.x0[q];
+      arr.dir[q] = -arr.dp[q];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) w.s.E = acc ? E : E0;
+  __syncthreads();
+  return acc;
+}
+
+// check_cell_shape (utils/cell.py:80-125), float32 with float64 sums.
+__device__ inline bool cell_valid(const float* c, int n, const JrMoveParams& mv) {
+  const float vol = fabsf(det3(c));
+  const float vpa = __fdiv_rn(vol, (float)n);
+  const float vc = __double2float_rn(pow((double)vol, (double)(1.0f / 3.0f)));
+  const int pr[3][3] = {{0, 1, 2}, {1, 2, 0}, {0, 2, 1}};
+  float amin = INFINITY;
+  for (int p = 0; p < 3; ++p) {
+    const float* a = c + 3 * pr[p][0];
+    const float* b = c + 3 * pr[p][1];
+    const float* e = c + 3 * pr[p][2];
+    float cr[3];
+    cr[0] = __fsub_rn(__fmul_rn(a[1], b[2]), __fmul_rn(a[2], b[1]));
+    cr[1] = __fsub_rn(__fmul_rn(a[2], b[0]), __fmul_rn(a[0], b[2]));
+    cr[2] = __fsub_rn(__fmul_rn(a[0], b[1]), __fmul_rn(a[1], b[0]));
+    double sq = 0.0;
+    for (int q = 0; q < 3; ++q) sq += (double)cr[q] * (double)cr[q];
+    const float nrm = __double2float_rn(sqrt(sq));
+    float cn[3];
+    for (int q = 0; q < 3; ++q) cn[q] = __fdiv_rn(cr[q], nrm);
+    double hd = (double)cn[0] * (double)e[0];
+    hd = hd + (double)cn[1] * (double)e[1];
+    hd = hd + (double)cn[2] * (double)e[2];
+    const float h = fabsf(__double2float_rn(hd));
+    const float ratio = __fdiv_rn(h, vc);
+    if (ratio < amin || isnan(ratio)) amin = ratio;
+  }
+  return (vpa <= mv.max_vpa) && (vpa >= mv.min_vpa) && (amin >= mv.min_aspect);
+}
+
+// Volume move (volume.py:49-109 + _common.py:16-93).  Returns acceptance and
+// the reject reason (priority energy > cell > prior).
+__device__ bool move_volume(const JrParams& P, Walker& w, Key key, float step,
+                            double emax, float pressure, const float* mu,
+                            int& reason) {
+  WalkShared& s = w.s;
+  const WalkArrays& arr = w.arr;
+  const int n = w.n;
+  const JrMoveParams& mv = P.moves;
+  const Key k1 = split(key, 0u), k2 = split(key, 1u);
+  const int cur = s.cur, tr = cur ^ 1;
+  const float* h = s.cc[cur].raw;
+  const float oldV = s.cc[cur].vol;
+  const float sn = __fmul_rn(step, (float)n);
+  const float dV = __fmul_rn(sn, normal(bits32(k1, 0u)));
+  const float newV = fabsf(__fadd_rn(oldV, dV));
+  const float ratio = __fdiv_rn(newV, oldV);
+  const float scale = __double2float_rn(pow((double)ratio, (double)(1.0f / 3.0f)));
+  float nc[9];
+  for (int q = 0; q < 9; ++q) nc[q] = __fmul_rn(h[q], scale);
+  if (threadIdx.x == 0) make_cell_ctx(nc, s.cc[tr], arr.T + tr * 3 * P.model.n_images, P.model);
+  const int n3 = 3 * n;
+  for (int q = threadIdx.x; q < n3; q += blockDim.x) {
+    float& x = pos_at(arr.xs, q);
+    arr.x0[q] = x;
+    x = __fmul_rn(x, scale);
+  }
+  __syncthreads();
+  double d0, d1;
+  const double En = ham_eval<false>(P, w, tr, pressure, mu, d0, d1);
+  const bool valid = cell_valid(nc, n, mv);
+  const float u = uniform01(bits32(k2, 0u));
+  bool prior_ok;
+  if (mv.flat_v_prior) {
+    prior_ok = u < 1.0f;
+  } else {
+    // min(1, ratio**N): lax.integer_pow's binary exponentiation, in float64
+    double acc = 1.0, b = (double)ratio;
+    bool first = true;
+    int y = n;
+    while (y > 0) {
+      if (y & 1) {
+        acc = first ? b : acc * b;
+        first = false;
+      }
+      y >>= 1;
+      if (y > 0) b = b * b;
+    }
+    const double pa = acc < 1.0 ? acc : 1.0;
+    prior_ok = (double)u < pa;
+  }
+  const bool energy_ok = En < emax;
+  const bool acc = energy_ok && valid && prior_ok;
+  reason = acc ? 0 : (!energy_ok ? 1 : (!valid ? 2 : 3));
+  if (!acc) {
+    for (int q = threadIdx.x; q < n3; q += blockDim.x) pos_at(arr.xs, q) = arr.x0[q];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && acc) {
+    s.cur = tr;
+    s.E = En;
+  }
+  __syncthreads();
+  return acc;
+}
+
+// alchemical_morph (alchemical.py:40-79).
+__device__ bool move_morph(const JrParams& P, Walker& w, Key key, double emax,
+                           float pressure, const float* mu) {
+  WalkShared& s = w.s;
+  const WalkArrays& arr = w.arr;
+  const int atom = randint(split(key, 0u), 0, w.n);
+  const int curt = __float_as_int(arr.xs[atom].w);
+  const int cand = randint(split(key, 1u), 0, P.model.n_species - 1);
+  const int nt = cand + (cand >= curt ? 1 : 0);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    arr.xs[atom].w = __int_as_float(nt);
+    s.counts[curt] -= 1;
+    s.counts[nt] += 1;
+  }
+  __syncthreads();
+  double d0, d1;
+  const double En = ham_eval<false>(P, w, s.cur, pressure, mu, d0, d1);
+  const bool acc = En < emax;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (acc) {
+      s.E = En;
+    } else {
+      arr.xs[atom].w = __int_as_float(curt);
+      s.counts[curt] += 1;
+      s.counts[nt] -= 1;
+    }
+  }
+  __syncthreads();
+  return acc;
+}
+
+// species_swap over all species (swap.py:177-260).
+__device__ bool move_swap(const JrParams& P, Walker& w, Key key, double emax,
+                          float pressure, const float* mu) {
+  WalkShared& s = w.s;
+  const WalkArrays& arr = w.arr;
+  const int n = w.n;
+  const int S = P.model.n_species;
+  const Key kp = split(key, 0u), klo = split(key, 1u), khi = split(key, 2u);
+  int counts[JR_MAX_SPECIES];
+  for (int q = 0; q < S; ++q) counts[q] = s.counts[q];
+  int plo[JR_MAX_SPECIES * JR_MAX_SPECIES], phi[JR_MAX_SPECIES * JR_MAX_SPECIES];
+  float cum[JR_MAX_SPECIES * JR_MAX_SPECIES];
+  int np = 0;
+  float total = 0.0f;
+  for (int a = 0; a < S; ++a)
+    for (int b = a + 1; b < S; ++b) {
+      plo[np] = a;
+      phi[np] = b;
+      total = __fadd_rn(total, (float)(counts[a] * counts[b]));
+      cum[np] = total;
+      ++np;
+    }
+  const bool has_pair = total > 0.0f;
+  const float u = __fmul_rn(uniform01(bits32(kp, 0u)), has_pair ? total : 1.0f);
+  int pidx = 0;
+  while (pidx < np && cum[pidx] <= u) ++pidx;
+  if (pidx > np - 1) pidx = np - 1;
+  const int clo = plo[pidx], chi = phi[pidx];
+  const int klo_i = randint(klo, 0, counts[clo] > 1 ? counts[clo] : 1);
+  const int khi_i = randint(khi, 0, counts[chi] > 1 ? counts[chi] : 1);
+  int ilo = n - 1, ihi = n - 1;
+  {
+    int run = 0;
+    for (int i = 0; i < n; ++i) {
+      run += (__float_as_int(arr.xs[i].w) == clo);
+      if (run >= klo_i + 1) { ilo = i; break; }
+    }
+    run = 0;
+    for (int i = 0; i < n; ++i) {
+      run += (__float_as_int(arr.xs[i].w) == chi);
+      if (run >= khi_i + 1) { ihi = i; break; }
+    }
+  }
+  const int tlo = __float_as_int(arr.xs[ilo].w), thi = __float_as_int(arr.xs[ihi].w);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    arr.xs[ilo].w = __int_as_float(chi);
+    arr.xs[ihi].w = __int_as_float(clo);
+  }
+  __syncthreads();
+  double d0, d1;
+  const double En = ham_eval<false>(P, w, s.cur, pressure, mu, d0, d1);
+  const bool acc = (En < emax) && has_pair;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (acc) {
+      s.E = En;
+    } else {
+      arr.xs[ilo].w = __int_as_float(tlo);
+      arr.xs[ihi].w = __int_as_float(thi);
+    }
+  }
+  __syncthreads();
+  return acc;
+}
+
+// One move of type P.moves.type[idx]; returns acceptance and reject reason.
+__device__ __forceinline__ bool run_move(const JrParams& P, Walker& w, int idx,
+                                         Key key, float step, double emax,
+                                         float pressure, const float* mu,
+                                         int& reason) {
+  reason = 0;
+  switch (P.moves.type[idx]) {
+    case JR_MOVE_GALILEAN:
+      return move_galilean(P, w, key, step, P.moves.n_reflect[idx],
+                           P.moves.perturb_angle[idx], emax, pressure, mu);
+    case JR_MOVE_VOLUME:
+      return move_volume(P, w, key, step, emax, pressure, mu, reason);
+    case JR_MOVE_MORPH:
+      return move_morph(P, w, key, emax, pressure, mu);
+    case JR_MOVE_SWAP: {
+      const bool a = move_swap(P, w, key, emax, pressure, mu);
+      reason = a ? 0 : 1;
+      return a;
+    }
+  }
+  return false;
+}
+
+// MWG step (mwg.py:227-257 with the _wrap counters of mwg.py:108-150) plus
+// the ns_step scan-body counters (nested_sampling.py:541-609).
+__device__ __forceinline__ void mwg_step(const JrParams& P, Walker& w, Key step_key,
+                                         Key move_key, double emax, float pressure,
+                                         const float* mu) {
+  WalkShared& s = w.s;
+  const int idx = choice(move_key, P.moves.cum_probs, P.moves.n_moves);
+  int reason = 0;
+  const bool acc = run_move(P, w, idx, step_key, s.step_sizes[idx], emax, pressure,
+                            mu, reason);
+  if (threadIdx.x == 0) {
+    s.w_prop[idx] += 1;
+    s.w_acc[idx] += acc ? 1 : 0;
+    s.c_prop[idx] += 1;
+    s.c_acc[idx] += acc ? 1 : 0;
+    const int col = acc ? 0 : (reason > 1 ? reason : 1);
+    s.c_rr[idx * 4 + col] += 1;
+    const bool gal = P.moves.type[idx] == JR_MOVE_GALILEAN;
+    const int ne = gal ? P.moves.n_reflect[idx] : 1;
+    s.c_nev[idx] += ne;
+    s.c_ngr[idx] += gal ? ne : 0;
+  }
+}
+
+// ------------------------------------------------------ load / store ----
+
+__device__ inline void load_tables(const JrParams& P, WalkShared& s) {
+  const int SS = P.model.n_species * P.model.n_species;
+  for (int q = threadIdx.x; q < SS; q += blockDim.x) {
+    s.sig2[q] = P.model.sig2[q];
+    s.eps4[q] = P.model.eps4[q];
+    s.eps24[q] = P.model.eps24[q];
+  }
+}
+
+// Load walker `slot` of replica p into smem.  zero_counters: a fresh clone
+// (nested_sampling.py:507-512).
+__device__ inline void load_walker(const JrParams& P, const JrDims& D,
+                                   const JrStateBuffers& st, Walker& w, int p,
+                                   int slot, bool zero_counters) {
+  WalkShared& s = w.s;
+  const WalkArrays& arr = w.arr;
+  const int n = w.n;
+  const int K = D.n_walkers, Nmax = D.n_atoms_max, M = D.n_moves;
+  const size_t wb = (size_t)p * K + slot;
+  const float* gx = st.positions + wb * Nmax * 3;
+  const float* gd = st.direction + wb * Nmax * 3;
+  const int32_t* gt = st.types + wb * Nmax;
+  __syncthreads();
+  for (int q = threadIdx.x; q < 3 * n; q += blockDim.x) {
+    pos_at(arr.xs, q) = gx[q];
+    arr.dir[q] = gd[q];
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) arr.xs[i].w = __int_as_float(gt[i]);
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < JR_MAX_SPECIES; ++q) s.counts[q] = 0;
+    s.E = st.energy64[wb];
+    for (int m = 0; m < M; ++m) {
+      s.step_sizes[m] = st.step_sizes[wb * M + m];
+      s.w_acc[m] = zero_counters ? 0 : st.n_accepted[wb * M + m];
+      s.w_prop[m] = zero_counters ? 0 : st.n_proposed[wb * M + m];
+    }
+    s.cur = 0;
+    make_cell_ctx(st.cell + wb * 9, s.cc[0], arr.T, P.model);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int i = 0; i < n; ++i) s.counts[__float_as_int(arr.xs[i].w)] += 1;
+  __syncthreads();
+}
+
+// Store the smem walker into `slot` of replica p.
+__device__ inline void store_walker(const JrDims& D, const JrStateBuffers& st,
+                                    Walker& w, int p, int slot) {
+  WalkShared& s = w.s;
+  const WalkArrays& arr = w.arr;
+  const int n = w.n;
+  const int K = D.n_walkers, Nmax = D.n_atoms_max, M = D.n_moves;
+  const size_t wb = (size_t)p * K + slot;
+  float* gx = st.positions + wb * Nmax * 3;
+  float* gd = st.direction + wb * Nmax * 3;
+  int32_t* gt = st.types + wb * Nmax;
+  __syncthreads();
+  for (int q = threadIdx.x; q < 3 * n; q += blockDim.x) {
+    gx[q] = pos_at(arr.xs, q);
+    gd[q] = arr.dir[q];
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) gt[i] = __float_as_int(arr.xs[i].w);
+  if (threadIdx.x == 0) {
+    st.energy64[wb] = s.E;
+    st.energy[wb] = __double2float_rn(s.E);
+    for (int q = 0; q < 9; ++q) st.cell[wb * 9 + q] = s.cc[s.cur].raw[q];
+    for (int m = 0; m < M; ++m) {
+      st.step_sizes[wb * M + m] = s.step_sizes[m];
+      st.n_accepted[wb * M + m] = s.w_acc[m];
+      st.n_proposed[wb * M + m] = s.w_prop[m];
+    }
+  }
+}
+
+__device__ inline void zero_chain_counters(WalkShared& s) {
+  if (threadIdx.x == 0) {
+    for (int m = 0; m < JR_MAX_MOVES; ++m) {
+      s.c_acc[m] = s.c_prop[m] = s.c_nev[m] = s.c_ngr[m] = 0;
+      s.c_rr[4 * m] = s.c_rr[4 * m + 1] = s.c_rr[4 * m + 2] = s.c_rr[4 * m + 3] = 0;
+    }
+  }
+}
+
+}  // namespace jr

@@ -1,0 +1,1174 @@
+/*
+ * jr_oracle.c -- CPU oracle for jaxrens's nested-sampling walk.
+ *
+ * TEST INFRASTRUCTURE ONLY.  tests/, the smoke check and bench.py's CPU
+ * baseline leg are the only callers; the product library never links it.
+ * See jr_oracle.h for the precision modes.  Every function cites the
+ * reference file:line it restates (paths relative to the jaxrens tree).
+ *
+ * Build with -ffp-contract=off: the FP32 arithmetic here must be exactly
+ * the sequence of IEEE operations written, with fmaf() only where an FMA is
+ * part of the kernel contract.
+ */
+#include "jr_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <pthread.h>
+
+/* ------------------------------------------------------------------ */
+/* threefry2x32-20 (Salmon et al., SC'11; Random123 threefry.h).       */
+/* JAX: jax._src.prng.threefry2x32 (dependency jax>=0.9, not vendored). */
+/* ------------------------------------------------------------------ */
+static inline uint32_t rotl32(uint32_t x, int r) {
+  return (x << r) | (x >> (32 - r));
+}
+
+void jro_threefry2x32(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1,
+                      uint32_t out[2]) {
+  static const int rot[8] = {13, 15, 26, 6, 17, 29, 16, 24};
+  const uint32_t ks[3] = {k0, k1, 0x1BD11BDAu ^ k0 ^ k1};
+  uint32_t x0 = c0 + ks[0];
+  uint32_t x1 = c1 + ks[1];
+  for (int r = 0; r < 20; ++r) {
+    x0 += x1;
+    x1 = rotl32(x1, rot[r & 7]);
+    x1 ^= x0;
+    if ((r & 3) == 3) {
+      const uint32_t s = (uint32_t)((r >> 2) + 1);
+      x0 += ks[s % 3];
+      x1 += ks[(s + 1) % 3] + s;
+    }
+  }
+  out[0] = x0;
+  out[1] = x1;
+}
+
+/* split(key, n)[index] with jax_threefry_partitionable=True: the counter of
+ * element i of shape (n,) is the 64-bit iota value i split as (hi, lo). */
+void jro_split(const uint32_t key[2], uint32_t index, uint32_t out[2]) {
+  jro_threefry2x32(key[0], key[1], 0u, index, out);
+}
+
+/* fold_in(key, d) = threefry_2x32(key, threefry_seed(d)) = hash(key,(0,d)). */
+void jro_fold_in(const uint32_t key[2], uint32_t data, uint32_t out[2]) {
+  jro_threefry2x32(key[0], key[1], 0u, data, out);
+}
+
+/* The pre-0.5 (non-partitionable) split: counts = iota(2n) hashed as the
+ * pairs (i, n+i); output words laid out [y0..., y1...] then reshaped (n,2).
+ * Kept only to pin the cipher against JAX's documented split(key(0)). */
+void jro_split_original(const uint32_t key[2], int32_t n, uint32_t* out) {
+  uint32_t* flat = (uint32_t*)malloc(sizeof(uint32_t) * 2 * (size_t)n);
+  for (int32_t i = 0; i < n; ++i) {
+    uint32_t y[2];
+    jro_threefry2x32(key[0], key[1], (uint32_t)i, (uint32_t)(n + i), y);
+    flat[i] = y[0];
+    flat[n + i] = y[1];
+  }
+  memcpy(out, flat, sizeof(uint32_t) * 2 * (size_t)n);
+  free(flat);
+}
+
+/* random_bits(key, 32, shape)[flat] (partitionable): bits1 ^ bits2. */
+uint32_t jro_bits32(const uint32_t key[2], uint32_t flat_index) {
+  uint32_t y[2];
+  jro_threefry2x32(key[0], key[1], 0u, flat_index, y);
+  return y[0] ^ y[1];
+}
+
+static inline float bits_to_unit(uint32_t bits) {
+  uint32_t b = (bits >> 9) | 0x3F800000u;
+  float f;
+  memcpy(&f, &b, 4);
+  return f - 1.0f;
+}
+
+/* jax.random.uniform (jax._src.random._uniform): mantissa fill, then
+ * floats * (maxval - minval) + minval, then max(minval, .). */
+float jro_uniform(uint32_t bits, float lo, float hi) {
+  float f = bits_to_unit(bits);
+  float span = hi - lo;
+  float r = f * span;
+  r = r + lo;
+  return r > lo ? r : lo;
+}
+
+/* XLA's float32 ErfInv: M. Giles, "Approximating the erfinv function",
+ * GPU Computing Gems Jade Edition (2011), single-precision branch with the
+ * polynomial evaluated as p = c_i + p*w (separate multiply and add).
+ * log1p is evaluated in double and rounded once, the same contract the
+ * kernels use, so CPU and GPU agree except at float rounding ties. */
+float jro_erfinv(float x) {
+  static const float lt5[9] = {2.81022636e-08f,  3.43273939e-07f,
+                               -3.5233877e-06f,  -4.39150654e-06f,
+                               0.00021858087f,   -0.00125372503f,
+                               -0.00417768164f,  0.246640727f,
+                               1.50140941f};
+  static const float ge5[9] = {-0.000200214257f, 0.000100950558f,
+                               0.00134934322f,   -0.00367342844f,
+                               0.00573950773f,   -0.0076224613f,
+                               0.00943887047f,   1.00167406f,
+                               2.83297682f};
+  float xx = x * x;
+  float w = -(float)log1p((double)(-xx));
+  float p;
+  if (w < 5.0f) {
+    w = w - 2.5f;
+    p = lt5[0];
+    for (int i = 1; i < 9; ++i) {
+      float pw = p * w;
+      p = lt5[i] + pw;
+    }
+  } else {
+    w = sqrtf(w) - 3.0f;
+    p = ge5[0];
+    for (int i = 1; i < 9; ++i) {
+      float pw = p * w;
+      p = ge5[i] + pw;
+    }
+  }
+  if (fabsf(x) == 1.0f) return x * FLT_MAX;
+  return p * x;
+}
+
+/* jax.random.normal (jax._src.random._normal_real):
+ * sqrt(2) * erf_inv(uniform(key, lo=nextafter(-1, 0), hi=1)). */
+float jro_normal(uint32_t bits) {
+  const float lo = nextafterf(-1.0f, 0.0f);
+  float u = jro_uniform(bits, lo, 1.0f);
+  return 1.41421354f * jro_erfinv(u);
+}
+
+/* jax.random.randint, int32, scalar shape (jax._src.random._randint). */
+int32_t jro_randint(const uint32_t key[2], int32_t lo, int32_t hi) {
+  uint32_t k1[2], k2[2];
+  jro_split(key, 0, k1);
+  jro_split(key, 1, k2);
+  uint32_t higher = jro_bits32(k1, 0);
+  uint32_t lower = jro_bits32(k2, 0);
+  uint32_t span = (uint32_t)(hi - lo);
+  if (hi <= lo) span = 1u;
+  uint32_t mult = 65536u % span;
+  mult = (uint32_t)(mult * mult) % span;
+  uint32_t off = (uint32_t)((higher % span) * mult + (lower % span));
+  off = off % span;
+  return lo + (int32_t)off;
+}
+
+/* jax.random.choice(key, m, p=p) with replace=True:
+ * r = cum[-1] * (1 - uniform(key)); index = searchsorted(cum, r, 'left'). */
+int32_t jro_choice(const uint32_t key[2], const float* cum, int32_t m) {
+  float u = bits_to_unit(jro_bits32(key, 0));
+  float one_minus = 1.0f - u;
+  float r = cum[m - 1] * one_minus;
+  int32_t idx = 0;
+  while (idx < m && cum[idx] < r) ++idx;
+  return idx;
+}
+
+void jro_normal_array(const uint32_t key[2], int32_t n, float* out) {
+  for (int32_t i = 0; i < n; ++i) out[i] = jro_normal(jro_bits32(key, (uint32_t)i));
+}
+
+void jro_uniform_array(const uint32_t key[2], int32_t n, float* out) {
+  for (int32_t i = 0; i < n; ++i)
+    out[i] = jro_uniform(jro_bits32(key, (uint32_t)i), 0.0f, 1.0f);
+}
+
+/* ------------------------------------------------------------------ */
+/* Geometry                                                            */
+/* ------------------------------------------------------------------ */
+
+/* jnp.linalg.det for 3x3 (jax._src.numpy.linalg._det_3x3), float32,
+ * evaluated left to right as written there. */
+float jro_det3(const float* a) {
+  float t1 = (a[0] * a[4]) * a[8];
+  float t2 = (a[1] * a[5]) * a[6];
+  float t3 = (a[2] * a[3]) * a[7];
+  float t4 = (a[2] * a[4]) * a[6];
+  float t5 = (a[0] * a[5]) * a[7];
+  float t6 = (a[1] * a[3]) * a[8];
+  float s = t1 + t2;
+  s = s + t3;
+  s = s - t4;
+  s = s - t5;
+  s = s - t6;
+  return s;
+}
+
+static int is_diag(const float* c) {
+  return c[1] == 0.0f && c[2] == 0.0f && c[3] == 0.0f && c[5] == 0.0f &&
+         c[6] == 0.0f && c[7] == 0.0f;
+}
+
+/* Kernel contract for inv(cell): a diagonal cell inverts element-wise with
+ * float32 division (what LU-solve produces for a diagonal matrix); any other
+ * cell uses the double adjugate divided by the double determinant, rounded
+ * once to float32.  The reference (lj.py:156) uses jnp.linalg.inv. */
+void jro_inv_cell(const float* c, float* inv) {
+  if (is_diag(c)) {
+    memset(inv, 0, 9 * sizeof(float));
+    inv[0] = 1.0f / c[0];
+    inv[4] = 1.0f / c[4];
+    inv[8] = 1.0f / c[8];
+    return;
+  }
+  double a[9];
+  for (int i = 0; i < 9; ++i) a[i] = (double)c[i];
+  double cof[9];
+  cof[0] = a[4] * a[8] - a[5] * a[7];
+  cof[1] = a[5] * a[6] - a[3] * a[8];
+  cof[2] = a[3] * a[7] - a[4] * a[6];
+  cof[3] = a[2] * a[7] - a[1] * a[8];
+  cof[4] = a[0] * a[8] - a[2] * a[6];
+  cof[5] = a[1] * a[6] - a[0] * a[7];
+  cof[6] = a[1] * a[5] - a[2] * a[4];
+  cof[7] = a[2] * a[3] - a[0] * a[5];
+  cof[8] = a[0] * a[4] - a[1] * a[3];
+  double det = a[0] * cof[0] + a[1] * cof[1] + a[2] * cof[2];
+  /* inv[i][j] = cof[j][i] / det */
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) inv[i * 3 + j] = (float)(cof[j * 3 + i] / det);
+}
+
+static void inv_cell_f64(const double* a, double* inv) {
+  double cof[9];
+  cof[0] = a[4] * a[8] - a[5] * a[7];
+  cof[1] = a[5] * a[6] - a[3] * a[8];
+  cof[2] = a[3] * a[7] - a[4] * a[6];
+  cof[3] = a[2] * a[7] - a[1] * a[8];
+  cof[4] = a[0] * a[8] - a[2] * a[6];
+  cof[5] = a[1] * a[6] - a[0] * a[7];
+  cof[6] = a[1] * a[5] - a[2] * a[4];
+  cof[7] = a[2] * a[3] - a[0] * a[5];
+  cof[8] = a[0] * a[4] - a[1] * a[3];
+  double det = a[0] * cof[0] + a[1] * cof[1] + a[2] * cof[2];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) inv[i * 3 + j] = cof[j * 3 + i] / det;
+}
+
+/* ------------------------------------------------------------------ */
+/* Lennard-Jones (backends/lj.py:125-204)                              */
+/* ------------------------------------------------------------------ */
+
+static int center_image(const JroModel* m) {
+  for (int k = 0; k < m->n_images; ++k)
+    if (m->img_off[3 * k] == 0.0f && m->img_off[3 * k + 1] == 0.0f &&
+        m->img_off[3 * k + 2] == 0.0f)
+      return k;
+  return -1;
+}
+
+/* DEV contract, one ordered pair: r2 by FMA chain, reciprocal, LJ powers. */
+static inline void dev_pair(const JroModel* m, int ti, int tj, float dx,
+                            float dy, float dz, float* e, float* g) {
+  float r2 = dx * dx;
+  r2 = fmaf(dy, dy, r2);
+  r2 = fmaf(dz, dz, r2);
+  if (m->has_cutoff && !(r2 < m->rc2)) {
+    *e = 0.0f;
+    *g = 0.0f;
+    return;
+  }
+  const int S = m->n_species;
+  float sig2 = m->sig2[ti * S + tj];
+  float eps4 = m->eps4[ti * S + tj];
+  float eps24 = m->eps24[ti * S + tj];
+  float ri = 1.0f / r2;
+  float s2 = sig2 * ri;
+  float s4 = s2 * s2;
+  float s6 = s4 * s2;
+  float s12 = s6 * s6;
+  float diff = s12 - s6;
+  *e = eps4 * diff;
+  float t = fmaf(2.0f, s12, -s6);
+  float a = eps24 * ri;
+  *g = -(a * t);
+}
+
+static double lj_dev(const JroModel* m, int n, const float* x,
+                     const int32_t* t, const float* cell_in, double* F) {
+  float safe[9];
+  const float* c = cell_in;
+  if (jro_det3(cell_in) == 0.0f) {
+    memset(safe, 0, sizeof(safe));
+    safe[0] = safe[4] = safe[8] = 1.0e10f;
+    c = safe;
+  }
+  float inv[9];
+  jro_inv_cell(c, inv);
+  const int nimg = m->n_images;
+  const int ctr = center_image(m);
+  float T[JRO_MAX_IMAGES * 3];
+  for (int k = 0; k < nimg; ++k) {
+    const float* o = m->img_off + 3 * k;
+    for (int q = 0; q < 3; ++q) {
+      float v = o[0] * c[q];
+      v = fmaf(o[1], c[3 + q], v);
+      v = fmaf(o[2], c[6 + q], v);
+      T[3 * k + q] = v;
+    }
+  }
+  double E = 0.0;
+  for (int i = 0; i < n; ++i) {
+    double fi[3] = {0.0, 0.0, 0.0};
+    for (int j = 0; j < n; ++j) {
+      float dr[3], d[3];
+      for (int q = 0; q < 3; ++q) dr[q] = x[3 * j + q] - x[3 * i + q];
+      float nn[3];
+      for (int q = 0; q < 3; ++q) {
+        float f = dr[0] * inv[q];
+        f = fmaf(dr[1], inv[3 + q], f);
+        f = fmaf(dr[2], inv[6 + q], f);
+        nn[q] = rintf(f);
+      }
+      for (int q = 0; q < 3; ++q) {
+        float s = nn[0] * c[q];
+        s = fmaf(nn[1], c[3 + q], s);
+        s = fmaf(nn[2], c[6 + q], s);
+        d[q] = dr[q] - s;
+      }
+      for (int k = 0; k < nimg; ++k) {
+        if (k == ctr && i == j) continue;
+        float dd[3];
+        if (nimg > 1) {
+          for (int q = 0; q < 3; ++q) dd[q] = d[q] + T[3 * k + q];
+        } else {
+          dd[0] = d[0]; dd[1] = d[1]; dd[2] = d[2];
+        }
+        float e, g;
+        dev_pair(m, t[i], t[j], dd[0], dd[1], dd[2], &e, &g);
+        E += (double)e;
+        if (F && i != j) {
+          for (int q = 0; q < 3; ++q) fi[q] += (double)(g * dd[q]);
+        }
+      }
+    }
+    if (F)
+      for (int q = 0; q < 3; ++q) F[3 * i + q] = (double)(float)fi[q];
+  }
+  return 0.5 * E;
+}
+
+/* REF32: the reference's float32 op order (no FMA, f32 row-major sums). */
+static double lj_ref32(const JroModel* m, int n, const float* x,
+                       const int32_t* t, const float* cell_in, double* F) {
+  float safe[9];
+  const float* c = cell_in;
+  if (jro_det3(cell_in) == 0.0f) {
+    memset(safe, 0, sizeof(safe));
+    safe[0] = safe[4] = safe[8] = 1.0e10f;
+    c = safe;
+  }
+  float inv[9];
+  jro_inv_cell(c, inv);
+  const int nimg = m->n_images;
+  const int ctr = center_image(m);
+  const int S = m->n_species;
+  float T[JRO_MAX_IMAGES * 3];
+  for (int k = 0; k < nimg; ++k) {
+    const float* o = m->img_off + 3 * k;
+    for (int q = 0; q < 3; ++q) {
+      float v = o[0] * c[q] + o[1] * c[3 + q];
+      v = v + o[2] * c[6 + q];
+      T[3 * k + q] = v;
+    }
+  }
+  float Esum = 0.0f;
+  float* Fs = NULL;
+  if (F) Fs = (float*)calloc((size_t)3 * n, sizeof(float));
+  for (int k = 0; k < nimg; ++k) {
+    for (int i = 0; i < n; ++i) {
+      for (int j = 0; j < n; ++j) {
+        float dr[3], d[3], nn[3];
+        for (int q = 0; q < 3; ++q) dr[q] = x[3 * j + q] - x[3 * i + q];
+        for (int q = 0; q < 3; ++q) {
+          float f = dr[0] * inv[q] + dr[1] * inv[3 + q];
+          f = f + dr[2] * inv[6 + q];
+          nn[q] = rintf(f);
+        }
+        for (int q = 0; q < 3; ++q) {
+          float s = nn[0] * c[q] + nn[1] * c[3 + q];
+          s = s + nn[2] * c[6 + q];
+          d[q] = dr[q] - s;
+        }
+        if (k == ctr && i == j) continue;
+        float dd[3];
+        for (int q = 0; q < 3; ++q) dd[q] = d[q] + T[3 * k + q];
+        float r2 = dd[0] * dd[0] + dd[1] * dd[1];
+        r2 = r2 + dd[2] * dd[2];
+        if (m->has_cutoff && !(r2 < m->rc2)) continue;
+        float sig2 = m->sig2[t[i] * S + t[j]];
+        float s2 = sig2 / r2;
+        float s6 = s2 * (s2 * s2);
+        float s12 = s6 * s6;
+        float e = m->eps4[t[i] * S + t[j]] * (s12 - s6);
+        Esum = Esum + e;
+        if (Fs && i != j) {
+          float coef = (m->eps24[t[i] * S + t[j]] / r2) * (2.0f * s12 - s6);
+          for (int q = 0; q < 3; ++q) Fs[3 * i + q] = Fs[3 * i + q] - coef * dd[q];
+        }
+      }
+    }
+  }
+  if (F) {
+    for (int i = 0; i < 3 * n; ++i) F[i] = (double)Fs[i];
+    free(Fs);
+  }
+  return (double)(0.5f * Esum);
+}
+
+/* Everything in double: the error yardstick for the FP32 paths. */
+static double lj_f64(const JroModel* m, int n, const float* x,
+                     const int32_t* t, const float* cell_in, double* F) {
+  double c[9], inv[9];
+  for (int i = 0; i < 9; ++i) c[i] = (double)cell_in[i];
+  if (jro_det3(cell_in) == 0.0f) {
+    memset(c, 0, sizeof(c));
+    c[0] = c[4] = c[8] = 1.0e10;
+  }
+  inv_cell_f64(c, inv);
+  const int nimg = m->n_images;
+  const int ctr = center_image(m);
+  const int S = m->n_species;
+  double T[JRO_MAX_IMAGES * 3];
+  for (int k = 0; k < nimg; ++k) {
+    const float* o = m->img_off + 3 * k;
+    for (int q = 0; q < 3; ++q)
+      T[3 * k + q] = o[0] * c[q] + o[1] * c[3 + q] + o[2] * c[6 + q];
+  }
+  double E = 0.0;
+  if (F) memset(F, 0, sizeof(double) * 3 * (size_t)n);
+  for (int i = 0; i < n; ++i) {
+    for (int j = 0; j < n; ++j) {
+      double dr[3], d[3], nn[3];
+      for (int q = 0; q < 3; ++q) dr[q] = (double)x[3 * j + q] - (double)x[3 * i + q];
+      for (int q = 0; q < 3; ++q)
+        nn[q] = nearbyint(dr[0] * inv[q] + dr[1] * inv[3 + q] + dr[2] * inv[6 + q]);
+      for (int q = 0; q < 3; ++q)
+        d[q] = dr[q] - (nn[0] * c[q] + nn[1] * c[3 + q] + nn[2] * c[6 + q]);
+      for (int k = 0; k < nimg; ++k) {
+        if (k == ctr && i == j) continue;
+        double dd[3];
+        for (int q = 0; q < 3; ++q) dd[q] = d[q] + T[3 * k + q];
+        double r2 = dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2];
+        if (m->has_cutoff && !(r2 < (double)m->rc2)) continue;
+        double sig2 = (double)m->sig2[t[i] * S + t[j]];
+        double eps4 = (double)m->eps4[t[i] * S + t[j]];
+        double s2 = sig2 / r2, s6 = s2 * s2 * s2, s12 = s6 * s6;
+        E += eps4 * (s12 - s6);
+        if (F && i != j) {
+          double coef = (6.0 * eps4 / r2) * (2.0 * s12 - s6);
+          for (int q = 0; q < 3; ++q) F[3 * i + q] -= coef * dd[q];
+        }
+      }
+    }
+  }
+  return 0.5 * E;
+}
+
+/* Gaussian-mixture toy (backends/toy.py:163-204), evaluated in double. */
+static double gauss_mix(const JroModel* m, int n, const float* x, double* F) {
+  double com[3] = {0, 0, 0};
+  for (int i = 0; i < n; ++i)
+    for (int q = 0; q < 3; ++q) com[q] += (double)x[3 * i + q];
+  for (int q = 0; q < 3; ++q) com[q] /= (double)n;
+  const double s2 = (double)m->gm_sigma * (double)m->gm_sigma;
+  const double lnorm = 1.5 * log(2.0 * M_PI * s2);
+  double l[JRO_MAX_CENTERS], lmax = -INFINITY;
+  for (int k = 0; k < m->n_centers; ++k) {
+    double ds = 0.0;
+    for (int q = 0; q < 3; ++q) {
+      double df = com[q] - (double)m->centers[3 * k + q];
+      ds += df * df;
+    }
+    l[k] = -0.5 * ds / s2 - lnorm;
+    if (l[k] > lmax) lmax = l[k];
+  }
+  double z = 0.0;
+  for (int k = 0; k < m->n_centers; ++k) z += exp(l[k] - lmax);
+  double E = -(lmax + log(z));
+  if (F) {
+    double gcom[3] = {0, 0, 0};
+    for (int k = 0; k < m->n_centers; ++k) {
+      double p = exp(l[k] - lmax) / z;
+      for (int q = 0; q < 3; ++q)
+        gcom[q] += p * (com[q] - (double)m->centers[3 * k + q]) / s2;
+    }
+    for (int i = 0; i < n; ++i)
+      for (int q = 0; q < 3; ++q) F[3 * i + q] = (double)(float)(-gcom[q] / (double)n);
+  }
+  return E;
+}
+
+/* EnsembleTerm (backends/ensemble.py:34-59) + Hamiltonian sum
+ * (backends/hamiltonian.py:112-153). */
+double jro_energy(const JroModel* mdl, int32_t mode, int32_t n, const float* x,
+                  const int32_t* types, const float* cell, float pressure,
+                  const float* mu, int32_t has_mu, double* forces,
+                  double* u_out) {
+  double U;
+  if (mdl->model == JRO_MODEL_GAUSS_MIX) {
+    U = gauss_mix(mdl, n, x, forces);
+  } else if (mode == JRO_DEV) {
+    U = lj_dev(mdl, n, x, types, cell, forces);
+  } else if (mode == JRO_REF32) {
+    U = lj_ref32(mdl, n, x, types, cell, forces);
+  } else {
+    U = lj_f64(mdl, n, x, types, cell, forces);
+  }
+  if (u_out) *u_out = U;
+  if (mdl->model == JRO_MODEL_GAUSS_MIX) return U;
+  int32_t counts[JRO_MAX_SPECIES] = {0};
+  for (int i = 0; i < n; ++i) counts[types[i]]++;
+  float V = fabsf(jro_det3(cell));
+  if (mode == JRO_REF32) {
+    float ens = pressure * V;
+    if (has_mu) {
+      float dot = 0.0f;
+      for (int s = 0; s < mdl->n_species; ++s) dot = dot + mu[s] * (float)counts[s];
+      ens = ens - dot;
+    }
+    return (double)((float)U + ens);
+  }
+  double ens = (double)pressure * (double)V;
+  if (has_mu) {
+    double dot = 0.0;
+    for (int s = 0; s < mdl->n_species; ++s) dot += (double)mu[s] * (double)counts[s];
+    ens = ens - dot;
+  }
+  return U + ens;
+}
+
+/* ------------------------------------------------------------------ */
+/* Move helpers                                                        */
+/* ------------------------------------------------------------------ */
+
+static float vnorm(const float* v, int n, int mode) {
+  if (mode == JRO_REF32) {
+    float s = 0.0f;
+    for (int i = 0; i < n; ++i) s = s + v[i] * v[i];
+    return sqrtf(s);
+  }
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) s += (double)v[i] * (double)v[i];
+  return (float)sqrt(s);
+}
+
+static void vnormalize(float* v, int n, int mode) {
+  float nv = vnorm(v, n, mode);
+  float den = nv > 1e-10f ? nv : 1e-10f;
+  for (int i = 0; i < n; ++i) v[i] = v[i] / den;
+}
+
+static double eval_energy(const JroModel* mdl, int mode, int n, const float* x,
+                          const int32_t* t, const float* cell, float P,
+                          const float* mu, int has_mu, double* F) {
+  return jro_energy(mdl, mode, n, x, t, cell, P, mu, has_mu, F, NULL);
+}
+
+/* Galilean move (sampling/moves/galilean.py:142-300). */
+static int move_galilean(const JroModel* mdl, int mode, const uint32_t key[2],
+                         float step, int R, float pa, double emax, int n,
+                         float* x, float* d, int32_t* t, float* cell,
+                         double* energy, float P, const float* mu, int has_mu) {
+  const int n3 = 3 * n;
+  uint32_t k_init[2], k_pert[2];
+  jro_split(key, 0, k_init);
+  jro_split(key, 1, k_pert);
+  float* v = (float*)malloc(sizeof(float) * n3);
+  float* x0 = (float*)malloc(sizeof(float) * n3);
+  float* dp = (float*)malloc(sizeof(float) * n3);
+  double* F = (double*)malloc(sizeof(double) * n3);
+  float* Ff = (float*)malloc(sizeof(float) * n3);
+  float dn = vnorm(d, n3, mode);
+  if (dn < 1e-8f) {
+    for (int i = 0; i < n3; ++i) v[i] = jro_normal(jro_bits32(k_init, (uint32_t)i));
+  } else {
+    for (int i = 0; i < n3; ++i) {
+      float z = jro_normal(jro_bits32(k_pert, (uint32_t)i));
+      if (mode == JRO_REF32) {
+        float noise = pa * z;
+        v[i] = d[i] + noise;
+      } else {
+        v[i] = fmaf(pa, z, d[i]);
+      }
+    }
+  }
+  vnormalize(v, n3, mode);
+  memcpy(x0, x, sizeof(float) * n3);
+  memcpy(dp, v, sizeof(float) * n3);
+  double E0 = *energy;
+  double E = E0;
+  for (int r = 0; r < R; ++r) {
+    for (int i = 0; i < n3; ++i) {
+      if (mode == JRO_REF32) {
+        float sv = step * v[i];
+        x[i] = x[i] + sv;
+      } else {
+        x[i] = fmaf(step, v[i], x[i]);
+      }
+    }
+    E = eval_energy(mdl, mode, n, x, t, cell, P, mu, has_mu, F);
+    if (isnan(E)) E = INFINITY;
+    if (E >= emax) {
+      for (int i = 0; i < n3; ++i) Ff[i] = (float)F[i];
+      if (mode == JRO_REF32) {
+        float fn = vnorm(Ff, n3, mode);
+        float den = fn > 1e-10f ? fn : 1e-10f;
+        float dot = 0.0f;
+        for (int i = 0; i < n3; ++i) Ff[i] = Ff[i] / den;
+        for (int i = 0; i < n3; ++i) dot = dot + Ff[i] * v[i];
+        float two = 2.0f * dot;
+        for (int i = 0; i < n3; ++i) v[i] = v[i] - two * Ff[i];
+      } else {
+        double sff = 0.0, sfd = 0.0;
+        for (int i = 0; i < n3; ++i) {
+          sff += (double)Ff[i] * (double)Ff[i];
+          sfd += (double)Ff[i] * (double)v[i];
+        }
+        double nrm = sqrt(sff);
+        if (nrm < 1e-10) nrm = 1e-10;
+        float coef = (float)(2.0 * sfd / (nrm * nrm));
+        for (int i = 0; i < n3; ++i) v[i] = fmaf(-coef, Ff[i], v[i]);
+      }
+    }
+  }
+  int acc = E < emax;
+  if (acc) {
+    *energy = E;
+    memcpy(d, v, sizeof(float) * n3);
+  } else {
+    memcpy(x, x0, sizeof(float) * n3);
+    *energy = E0;
+    for (int i = 0; i < n3; ++i) d[i] = -dp[i];
+  }
+  free(v); free(x0); free(dp); free(F); free(Ff);
+  return acc;
+}
+
+/* utils/cell.py:80-125 check_cell_shape (float32; reductions per contract) */
+static int cell_valid(const float* c, int n, float max_vpa, float min_vpa,
+                      float min_aspect, int mode) {
+  float vol = fabsf(jro_det3(c));
+  float vpa = vol / (float)n;
+  float vc = (float)pow((double)vol, (double)(1.0f / 3.0f));
+  static const int pr[3][3] = {{0, 1, 2}, {1, 2, 0}, {0, 2, 1}};
+  float amin = INFINITY;
+  for (int p = 0; p < 3; ++p) {
+    const float* a = c + 3 * pr[p][0];
+    const float* b = c + 3 * pr[p][1];
+    const float* e = c + 3 * pr[p][2];
+    float cr[3];
+    cr[0] = a[1] * b[2] - a[2] * b[1];
+    cr[1] = a[2] * b[0] - a[0] * b[2];
+    cr[2] = a[0] * b[1] - a[1] * b[0];
+    float nrm = vnorm(cr, 3, mode);
+    float cn[3] = {cr[0] / nrm, cr[1] / nrm, cr[2] / nrm};
+    float h;
+    if (mode == JRO_REF32) {
+      h = cn[0] * e[0] + cn[1] * e[1];
+      h = h + cn[2] * e[2];
+    } else {
+      h = (float)((double)cn[0] * e[0] + (double)cn[1] * e[1] + (double)cn[2] * e[2]);
+    }
+    h = fabsf(h);
+    float ratio = h / vc;
+    if (ratio < amin || isnan(ratio)) amin = ratio;
+  }
+  return (vpa <= max_vpa) && (vpa >= min_vpa) && (amin >= min_aspect);
+}
+
+/* Volume move (sampling/moves/volume.py:49-109, moves/_common.py:16-93). */
+static int move_volume(const JroModel* mdl, const JroMoves* mv, int mode,
+                       const uint32_t key[2], float step, double emax, int n,
+                       float* x, int32_t* t, float* cell, double* energy,
+                       float P, const float* mu, int has_mu, int* reason) {
+  uint32_t k1[2], k2[2];
+  jro_split(key, 0, k1);
+  jro_split(key, 1, k2);
+  float oldV = fabsf(jro_det3(cell));
+  float sn = step * (float)n;
+  float dV = sn * jro_normal(jro_bits32(k1, 0));
+  float newV = fabsf(oldV + dV);
+  float ratio = newV / oldV;
+  float scale = (float)pow((double)ratio, (double)(1.0f / 3.0f));
+  float nc[9];
+  for (int i = 0; i < 9; ++i) nc[i] = cell[i] * scale;
+  float* nx = (float*)malloc(sizeof(float) * 3 * n);
+  for (int i = 0; i < 3 * n; ++i) nx[i] = x[i] * scale;
+  double En = eval_energy(mdl, mode, n, nx, t, nc, P, mu, has_mu, NULL);
+  int valid = cell_valid(nc, n, mv->max_vpa, mv->min_vpa, mv->min_aspect, mode);
+  int prior_ok;
+  float u = jro_uniform(jro_bits32(k2, 0), 0.0f, 1.0f);
+  if (mv->flat_v_prior) {
+    prior_ok = u < 1.0f;
+  } else if (mode == JRO_REF32) {
+    /* lax.integer_pow by binary exponentiation, float32 */
+    float acc = 1.0f, b = ratio;
+    int first = 1, y = n;
+    while (y > 0) {
+      if (y & 1) { acc = first ? b : acc * b; first = 0; }
+      y >>= 1;
+      if (y > 0) b = b * b;
+    }
+    float pa = acc < 1.0f ? acc : 1.0f;
+    prior_ok = u < pa;
+  } else {
+    double acc = 1.0, b = (double)ratio;
+    int first = 1, y = n;
+    while (y > 0) {
+      if (y & 1) { acc = first ? b : acc * b; first = 0; }
+      y >>= 1;
+      if (y > 0) b = b * b;
+    }
+    double pa = acc < 1.0 ? acc : 1.0;
+    prior_ok = (double)u < pa;
+  }
+  int energy_ok = En < emax;
+  int acc = energy_ok && valid && prior_ok;
+  *reason = acc ? 0 : (!energy_ok ? 1 : (!valid ? 2 : 3));
+  if (acc) {
+    memcpy(cell, nc, sizeof(nc));
+    memcpy(x, nx, sizeof(float) * 3 * n);
+    *energy = En;
+  }
+  free(nx);
+  return acc;
+}
+
+/* alchemical_morph (sampling/moves/alchemical.py:40-79). */
+static int move_morph(const JroModel* mdl, int mode, const uint32_t key[2],
+                      double emax, int n, float* x, int32_t* t, float* cell,
+                      double* energy, float P, const float* mu, int has_mu) {
+  uint32_t ka[2], ks[2];
+  jro_split(key, 0, ka);
+  jro_split(key, 1, ks);
+  int atom = jro_randint(ka, 0, n);
+  int cur = t[atom];
+  int cand = jro_randint(ks, 0, mdl->n_species - 1);
+  int nt = cand + (cand >= cur ? 1 : 0);
+  int32_t* tt = (int32_t*)malloc(sizeof(int32_t) * n);
+  memcpy(tt, t, sizeof(int32_t) * n);
+  tt[atom] = nt;
+  double En = eval_energy(mdl, mode, n, x, tt, cell, P, mu, has_mu, NULL);
+  int acc = En < emax;
+  if (acc) {
+    memcpy(t, tt, sizeof(int32_t) * n);
+    *energy = En;
+  }
+  free(tt);
+  return acc;
+}
+
+/* species_swap over every species (sampling/moves/swap.py:177-260). */
+static int move_swap(const JroModel* mdl, int mode, const uint32_t key[2],
+                     double emax, int n, float* x, int32_t* t, float* cell,
+                     double* energy, float P, const float* mu, int has_mu) {
+  const int S = mdl->n_species;
+  uint32_t kp[2], klo[2], khi[2];
+  jro_split(key, 0, kp);
+  jro_split(key, 1, klo);
+  jro_split(key, 2, khi);
+  int counts[JRO_MAX_SPECIES] = {0};
+  for (int i = 0; i < n; ++i) counts[t[i]]++;
+  int plo[JRO_MAX_SPECIES * JRO_MAX_SPECIES], phi[JRO_MAX_SPECIES * JRO_MAX_SPECIES];
+  int np = 0;
+  for (int a = 0; a < S; ++a)
+    for (int b = 0; b < S; ++b)
+      if (a < b) { plo[np] = a; phi[np] = b; ++np; }
+  float cum[JRO_MAX_SPECIES * JRO_MAX_SPECIES];
+  float total = 0.0f;
+  for (int p = 0; p < np; ++p) {
+    float w = (float)(counts[plo[p]] * counts[phi[p]]);
+    total = total + w;
+    cum[p] = total;
+  }
+  int has_pair = total > 0.0f;
+  float u = jro_uniform(jro_bits32(kp, 0), 0.0f, 1.0f) * (has_pair ? total : 1.0f);
+  int pidx = 0;
+  while (pidx < np && cum[pidx] <= u) ++pidx; /* searchsorted side='right' */
+  if (pidx > np - 1) pidx = np - 1;
+  int clo = plo[pidx], chi = phi[pidx];
+  int klo_i = jro_randint(klo, 0, counts[clo] > 1 ? counts[clo] : 1);
+  int khi_i = jro_randint(khi, 0, counts[chi] > 1 ? counts[chi] : 1);
+  int ilo = n - 1, ihi = n - 1, run = 0;
+  for (int i = 0; i < n; ++i) {
+    run += (t[i] == clo);
+    if (run >= klo_i + 1) { ilo = i; break; }
+  }
+  run = 0;
+  for (int i = 0; i < n; ++i) {
+    run += (t[i] == chi);
+    if (run >= khi_i + 1) { ihi = i; break; }
+  }
+  int32_t* tt = (int32_t*)malloc(sizeof(int32_t) * n);
+  memcpy(tt, t, sizeof(int32_t) * n);
+  tt[ilo] = chi;
+  tt[ihi] = clo;
+  double En = eval_energy(mdl, mode, n, x, tt, cell, P, mu, has_mu, NULL);
+  int acc = (En < emax) && has_pair;
+  if (acc) {
+    memcpy(t, tt, sizeof(int32_t) * n);
+    *energy = En;
+  }
+  free(tt);
+  return acc;
+}
+
+static double round_energy(double e, int mode) {
+  return mode == JRO_REF32 ? (double)(float)e : e;
+}
+
+int32_t jro_move_trial(const JroModel* mdl, const JroMoves* mv, int32_t mode,
+                       int32_t move_idx, const uint32_t key[2], float step,
+                       double emax, int32_t n, float* x, float* d, int32_t* t,
+                       float* cell, double* energy, float P, const float* mu,
+                       int32_t has_mu, int32_t* reason_out) {
+  int reason = 0, acc = 0;
+  switch (mv->type[move_idx]) {
+    case JRO_MOVE_GALILEAN:
+      acc = move_galilean(mdl, mode, key, step, mv->n_reflect[move_idx],
+                          mv->perturb_angle[move_idx], emax, n, x, d, t, cell,
+                          energy, P, mu, has_mu);
+      break;
+    case JRO_MOVE_VOLUME:
+      acc = move_volume(mdl, mv, mode, key, step, emax, n, x, t, cell, energy,
+                        P, mu, has_mu, &reason);
+      break;
+    case JRO_MOVE_MORPH:
+      acc = move_morph(mdl, mode, key, emax, n, x, t, cell, energy, P, mu, has_mu);
+      break;
+    case JRO_MOVE_SWAP:
+      acc = move_swap(mdl, mode, key, emax, n, x, t, cell, energy, P, mu, has_mu);
+      reason = acc ? 0 : 1;
+      break;
+  }
+  *energy = round_energy(*energy, mode);
+  if (reason_out) *reason_out = reason;
+  return acc;
+}
+
+/* build_mwg.step_fn (sampling/mwg.py:227-257) + _wrap (mwg.py:108-150). */
+int32_t jro_mwg_step(const JroModel* mdl, const JroMoves* mv, int32_t mode,
+                     const uint32_t step_key[2], const uint32_t move_key[2],
+                     double emax, int32_t n, float* x, float* d, int32_t* t,
+                     float* cell, double* energy, const float* step_sizes,
+                     int32_t* n_acc, int32_t* n_prop, float P, const float* mu,
+                     int32_t has_mu, int32_t* move_idx_out, int32_t* reason_out,
+                     int32_t* n_evals_out, int32_t* n_grad_out) {
+  int idx = jro_choice(move_key, mv->cum_probs, mv->n_moves);
+  int reason = 0;
+  int acc = jro_move_trial(mdl, mv, mode, idx, step_key, step_sizes[idx], emax,
+                           n, x, d, t, cell, energy, P, mu, has_mu, &reason);
+  n_prop[idx] += 1;
+  n_acc[idx] += acc;
+  *move_idx_out = idx;
+  *reason_out = reason;
+  int ne = 1, ng = 0;
+  if (mv->type[idx] == JRO_MOVE_GALILEAN) { ne = mv->n_reflect[idx]; ng = ne; }
+  *n_evals_out = ne;
+  *n_grad_out = ng;
+  return acc;
+}
+
+/* ------------------------------------------------------------------ */
+/* ns_step (sampling/nested_sampling.py:391-686), n_cull = 1            */
+/* ------------------------------------------------------------------ */
+
+static double logaddexp(double a, double b) {
+  double amax = a > b ? a : b;
+  double delta = a - b;
+  if (isnan(delta)) return a + b;
+  return amax + log1p(exp(-fabs(delta)));
+}
+
+static void copy_walker(JroReplica* r, int dst, int src, int M) {
+  const int N = r->n_atoms;
+  memcpy(r->positions + (size_t)dst * 3 * N, r->positions + (size_t)src * 3 * N, sizeof(float) * 3 * N);
+  memcpy(r->direction + (size_t)dst * 3 * N, r->direction + (size_t)src * 3 * N, sizeof(float) * 3 * N);
+  memcpy(r->types + (size_t)dst * N, r->types + (size_t)src * N, sizeof(int32_t) * N);
+  memcpy(r->cell + (size_t)dst * 9, r->cell + (size_t)src * 9, sizeof(float) * 9);
+  memcpy(r->step_sizes + (size_t)dst * M, r->step_sizes + (size_t)src * M, sizeof(float) * M);
+  r->energy[dst] = r->energy[src];
+}
+
+void jro_ns_step(const JroModel* mdl, const JroMoves* mv, int32_t mode,
+                 JroReplica* rep, int32_t T, int32_t n_extra,
+                 const uint32_t* move_key_in, double log_alpha, double w_offset,
+                 JroIterInfo* info, float* dead_x, int32_t* dead_t,
+                 float* dead_c) {
+  const int K = rep->n_walkers, N = rep->n_atoms, M = mv->n_moves;
+  uint32_t key[2] = {rep->rng_key[0], rep->rng_key[1]};
+  uint32_t k_a[2], k_worst[2], k_next[2], k_clone[2], k_extra[2], k_mcmc[2], k_moves[2];
+  jro_split(key, 0, k_a);
+  jro_split(key, 1, k_worst);
+  jro_split(k_a, 0, k_next);
+  jro_split(k_a, 1, k_clone);
+  jro_split(k_a, 2, k_extra);
+  jro_split(k_a, 3, k_mcmc);
+  jro_split(k_a, 4, k_moves);
+  uint32_t move_key[2];
+  if (move_key_in) { move_key[0] = move_key_in[0]; move_key[1] = move_key_in[1]; }
+  else { move_key[0] = k_moves[0]; move_key[1] = k_moves[1]; }
+
+  /* _find_worst_walker (nested_sampling.py:86-109): jnp.max propagates NaN */
+  double emax = rep->energy[0];
+  int any_nan = 0;
+  for (int k = 0; k < K; ++k) {
+    if (isnan(rep->energy[k])) any_nan = 1;
+    if (rep->energy[k] > emax) emax = rep->energy[k];
+  }
+  if (any_nan) emax = NAN;
+  int worst = 0;
+  float best = -INFINITY;
+  int found = 0;
+  for (int k = 0; k < K; ++k) {
+    if (rep->energy[k] == emax) {
+      float nz = jro_uniform(jro_bits32(k_worst, (uint32_t)k), 0.0f, 1.0f);
+      if (!found || nz > best) { best = nz; worst = k; found = 1; }
+    }
+  }
+  /* clone (nested_sampling.py:182-183) */
+  int clone = jro_randint(k_clone, 0, K - 1);
+  if (clone >= worst) clone += 1;
+  /* extras (nested_sampling.py:112-133): stable argsort of -noise */
+  int W = 1 + n_extra;
+  int* walk = (int*)malloc(sizeof(int) * W);
+  walk[0] = worst;
+  if (n_extra > 0) {
+    float* nz = (float*)malloc(sizeof(float) * K);
+    for (int k = 0; k < K; ++k) nz[k] = jro_uniform(jro_bits32(k_extra, (uint32_t)k), 0.0f, 1.0f);
+    nz[worst] = -INFINITY;
+    nz[clone] = -INFINITY;
+    char* used = (char*)calloc(K, 1);
+    for (int e = 0; e < n_extra; ++e) {
+      int bi = -1;
+      for (int k = 0; k < K; ++k)
+        if (!used[k] && (bi < 0 || nz[k] > nz[bi])) bi = k;
+      used[bi] = 1;
+      walk[1 + e] = bi;
+    }
+    free(used);
+    free(nz);
+  }
+  /* dead walker + evidence (nested_sampling.py:486-501) */
+  double dead_E = rep->energy[worst];
+  if (dead_x) memcpy(dead_x, rep->positions + (size_t)worst * 3 * N, sizeof(float) * 3 * N);
+  if (dead_t) memcpy(dead_t, rep->types + (size_t)worst * N, sizeof(int32_t) * N);
+  if (dead_c) memcpy(dead_c, rep->cell + (size_t)worst * 9, sizeof(float) * 9);
+  double lw = (double)(*rep->iteration) * log_alpha + w_offset;
+  *rep->log_evidence = logaddexp(*rep->log_evidence, lw - dead_E);
+  /* clone into the culled slot, counters reset (nested_sampling.py:504-518) */
+  copy_walker(rep, worst, clone, M);
+  for (int m = 0; m < M; ++m) {
+    rep->n_acc[(size_t)worst * M + m] = 0;
+    rep->n_prop[(size_t)worst * M + m] = 0;
+  }
+  memset(info, 0, sizeof(*info));
+  info->worst_idx = worst;
+  info->clone_idx = clone;
+  info->emax = emax;
+  info->dead_energy = dead_E;
+  /* walk W chains of T steps (nested_sampling.py:524-628) */
+  for (int w = 0; w < W; ++w) {
+    uint32_t ck[2];
+    jro_split(k_mcmc, (uint32_t)w, ck);
+    const int s = walk[w];
+    float* x = rep->positions + (size_t)s * 3 * N;
+    float* d = rep->direction + (size_t)s * 3 * N;
+    int32_t* t = rep->types + (size_t)s * N;
+    float* c = rep->cell + (size_t)s * 9;
+    for (int step = 0; step < T; ++step) {
+      uint32_t sk[2], mk[2];
+      jro_split(ck, (uint32_t)step, sk);
+      jro_split(move_key, (uint32_t)step, mk);
+      int midx, reason, ne, ng;
+      int acc = jro_mwg_step(mdl, mv, mode, sk, mk, emax, N, x, d, t, c,
+                             &rep->energy[s], rep->step_sizes + (size_t)s * M,
+                             rep->n_acc + (size_t)s * M, rep->n_prop + (size_t)s * M,
+                             rep->pressure, rep->mu, rep->has_mu, &midx, &reason,
+                             &ne, &ng);
+      info->n_acc[midx] += acc;
+      info->n_prop[midx] += 1;
+      int col = acc ? 0 : (reason > 1 ? reason : 1);
+      info->rr[midx * 4 + col] += 1;
+      info->n_evals[midx] += ne;
+      info->n_grad[midx] += ng;
+      info->total_accepted += acc;
+    }
+  }
+  free(walk);
+  *rep->emax = emax;
+  *rep->iteration += 1;
+  rep->rng_key[0] = k_next[0];
+  rep->rng_key[1] = k_next[1];
+}
+
+typedef struct {
+  const JroModel* mdl; const JroMoves* mv; int32_t mode; JroReplica* reps;
+  int32_t n_reps, T, n_extra; const uint32_t* mk; double log_alpha, w_offset;
+  JroIterInfo* infos; int32_t stride, first;
+} BatchArg;
+
+static void* batch_worker(void* p) {
+  BatchArg* a = (BatchArg*)p;
+  for (int r = a->first; r < a->n_reps; r += a->stride)
+    jro_ns_step(a->mdl, a->mv, a->mode, &a->reps[r], a->T, a->n_extra, a->mk,
+                a->log_alpha, a->w_offset, &a->infos[r], NULL, NULL, NULL);
+  return NULL;
+}
+
+/* Replicas are independent within one iteration: one pthread per slice. */
+void jro_ns_step_batched(const JroModel* mdl, const JroMoves* mv, int32_t mode,
+                         JroReplica* reps, int32_t n_reps, int32_t T,
+                         int32_t n_extra, int32_t shared_move_key,
+                         double log_alpha, double w_offset, JroIterInfo* infos,
+                         int32_t n_threads) {
+  uint32_t mk[2];
+  if (shared_move_key) jro_fold_in(reps[0].rng_key, 1u, mk);
+  int nt = n_threads > 0 ? n_threads : 1;
+  if (nt > n_reps) nt = n_reps;
+  if (nt > 256) nt = 256;
+  pthread_t th[256];
+  BatchArg args[256];
+  for (int i = 0; i < nt; ++i) {
+    BatchArg a = {mdl, mv, mode, reps, n_reps, T, n_extra,
+                  shared_move_key ? mk : NULL, log_alpha, w_offset, infos, nt, i};
+    args[i] = a;
+  }
+  for (int i = 1; i < nt; ++i) pthread_create(&th[i], NULL, batch_worker, &args[i]);
+  batch_worker(&args[0]);
+  for (int i = 1; i < nt; ++i) pthread_join(th[i], NULL);
+}
+
+/* ------------------------------------------------------------------ */
+/* Pressure / semi-grand replica exchange                              */
+/* (sampling/moves/replica_exchange.py:318-436, EnsembleSwap :120-156) */
+/* ------------------------------------------------------------------ */
+
+static double ens_energy(const JroReplica* r, const float* cell,
+                         const int32_t* t, int n, int S, int mode) {
+  int32_t counts[JRO_MAX_SPECIES] = {0};
+  for (int i = 0; i < n; ++i) counts[t[i]]++;
+  float V = fabsf(jro_det3(cell));
+  if (mode == JRO_REF32) {
+    float e = r->pressure * V;
+    if (r->has_mu) {
+      float dot = 0.0f;
+      for (int s = 0; s < S; ++s) dot = dot + r->mu[s] * (float)counts[s];
+      e = e - dot;
+    }
+    return (double)e;
+  }
+  double e = (double)r->pressure * (double)V;
+  if (r->has_mu) {
+    double dot = 0.0;
+    for (int s = 0; s < S; ++s) dot += (double)r->mu[s] * (double)counts[s];
+    e = e - dot;
+  }
+  return e;
+}
+
+static double rebase(double E, const JroReplica* from, const JroReplica* to,
+                     const float* cell, const int32_t* t, int n, int S, int mode) {
+  double u = E - ens_energy(from, cell, t, n, S, mode);
+  if (mode == JRO_REF32) u = (double)(float)u;
+  double out = u + ens_energy(to, cell, t, n, S, mode);
+  if (mode == JRO_REF32) out = (double)(float)out;
+  return out;
+}
+
+static void swap_slot(JroReplica* a, int wa, JroReplica* b, int wb, double Ea,
+                      double Eb) {
+  const int N = a->n_atoms;
+  float tx[3 * 1024];
+  int32_t tt[1024];
+  float tc[9];
+  /* positions */
+  memcpy(tx, a->positions + (size_t)wa * 3 * N, sizeof(float) * 3 * N);
+  memcpy(a->positions + (size_t)wa * 3 * N, b->positions + (size_t)wb * 3 * N, sizeof(float) * 3 * N);
+  memcpy(b->positions + (size_t)wb * 3 * N, tx, sizeof(float) * 3 * N);
+  memcpy(tx, a->direction + (size_t)wa * 3 * N, sizeof(float) * 3 * N);
+  memcpy(a->direction + (size_t)wa * 3 * N, b->direction + (size_t)wb * 3 * N, sizeof(float) * 3 * N);
+  memcpy(b->direction + (size_t)wb * 3 * N, tx, sizeof(float) * 3 * N);
+  memcpy(tt, a->types + (size_t)wa * N, sizeof(int32_t) * N);
+  memcpy(a->types + (size_t)wa * N, b->types + (size_t)wb * N, sizeof(int32_t) * N);
+  memcpy(b->types + (size_t)wb * N, tt, sizeof(int32_t) * N);
+  memcpy(tc, a->cell + (size_t)wa * 9, sizeof(tc));
+  memcpy(a->cell + (size_t)wa * 9, b->cell + (size_t)wb * 9, sizeof(tc));
+  memcpy(b->cell + (size_t)wb * 9, tc, sizeof(tc));
+  a->energy[wa] = Ea;
+  b->energy[wb] = Eb;
+}
+
+void jro_re_step(JroReplica* reps, int32_t R, const uint32_t key[2],
+                 int32_t n_cycles, int32_t mode, int32_t* acc_pp,
+                 int32_t* att_pp) {
+  if (R < 2) return;
+  const int K = reps[0].n_walkers;
+  const int n_even = (R - 1 + 1) / 2;       /* len(range(0, R-1, 2)) */
+  const int n_odd = (R - 1) / 2;            /* len(range(1, R-1, 2)) */
+  const int max_pairs = n_even > n_odd ? n_even : n_odd;
+  for (int p = 0; p < R - 1; ++p) { acc_pp[p] = 0; att_pp[p] = 0; }
+  for (int cyc = 0; cyc < n_cycles; ++cyc) {
+    uint32_t ck[2];
+    jro_split(key, (uint32_t)cyc, ck);
+    for (int phase = 0; phase < 2; ++phase) {
+      uint32_t pk[2];
+      jro_split(ck, (uint32_t)phase, pk);
+      const int n_valid = phase == 0 ? n_even : n_odd;
+      for (int slot = 0; slot < max_pairs; ++slot) {
+        uint32_t sk[2], k1[2], k2[2];
+        jro_split(pk, (uint32_t)slot, sk);
+        jro_split(sk, 0, k1);
+        jro_split(sk, 1, k2);
+        const int valid = slot < n_valid;
+        const int ri = valid ? phase + 2 * slot : 0;
+        const int rj = valid ? ri + 1 : 0;
+        int wi = jro_randint(k1, 0, K);
+        int wj = jro_randint(k2, 0, K);
+        if (!valid) continue; /* padding entries never swap */
+        JroReplica* A = &reps[ri];
+        JroReplica* B = &reps[rj];
+        const int N = A->n_atoms;
+        int S = JRO_MAX_SPECIES;
+        /* into_i = walker_j rebased into run i; into_j symmetric */
+        double into_i = rebase(B->energy[wj], B, A, B->cell + (size_t)wj * 9,
+                               B->types + (size_t)wj * N, N, S, mode);
+        double into_j = rebase(A->energy[wi], A, B, A->cell + (size_t)wi * 9,
+                               A->types + (size_t)wi * N, N, S, mode);
+        int do_swap = (into_i < *A->emax) && (into_j < *B->emax);
+        if (do_swap) swap_slot(A, wi, B, wj, into_i, into_j);
+        acc_pp[ri] += do_swap;
+        att_pp[ri] += 1;
+      }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* Synthetic uniform-gas initial walkers                               */
+/* ------------------------------------------------------------------ */
+void jro_init_walkers(const uint32_t key[2], int32_t K, int32_t N, float v_hi,
+                      float* positions, float* cell) {
+  for (int k = 0; k < K; ++k) {
+    uint32_t wk[2], kv[2], kp[2];
+    jro_split(key, (uint32_t)k, wk);
+    jro_split(wk, 0, kv);
+    jro_split(wk, 1, kp);
+    float u = jro_uniform(jro_bits32(kv, 0), 0.0f, 1.0f);
+    float V = v_hi * (1.0f - u);
+    float L = (float)pow((double)V, (double)(1.0f / 3.0f));
+    float* c = cell + (size_t)k * 9;
+    memset(c, 0, 9 * sizeof(float));
+    c[0] = c[4] = c[8] = L;
+    for (int i = 0; i < 3 * N; ++i) {
+      float f = jro_uniform(jro_bits32(kp, (uint32_t)i), 0.0f, 1.0f);
+      positions[(size_t)k * 3 * N + i] = f * L;
+    }
+  }
+}
