@@ -188,7 +188,7 @@ def run_ours(args):
                    "jr_autotune")
         cfg = best
     elif args.cluster is not None:
-        cfg = _lib.JrLaunchConfig(args.threads, args.tpa, args.cluster)
+        cfg = _lib.JrLaunchConfig(args.threads, args.tpa, args.cluster, int(args.warp))
     # prologue: leave the random-gas start before measuring (untimed)
     info = nsm.InfoBuffers(ns, step.n_moves, RE_INTERVAL, dead=True)
     for _ in range(args.prologue // RE_INTERVAL):
@@ -260,7 +260,8 @@ def run_ours(args):
         "config": dict(CONFIG, parallelism=f"replicas x{world} GPUs",
                        l2="flushed (256 MiB write) between timed steps",
                        launch=None if cfg is None else {"threads": cfg.threads, "tpa": cfg.tpa,
-                                                         "cluster": cfg.cluster}),
+                                                         "cluster": cfg.cluster,
+                                                         "warp_walkers": cfg.warp_walkers}),
         "ns_iters_per_s": ns_iters, "ns_iters_per_s_per_run": ns_iters / (world * P_RUNS),
         "e2e": e2e,
         "gpu_launches": 2 * args.steps,
@@ -385,6 +386,7 @@ def main():
     ap.add_argument("--cluster", type=int, default=None)
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--tpa", type=int, default=8)
+    ap.add_argument("--warp", type=int, default=0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

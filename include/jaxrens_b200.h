@@ -155,13 +155,15 @@ typedef struct JrInfoBuffers {
 } JrInfoBuffers;
 
 /* Launch shape of the walk kernels.  threads: CTA size; tpa: threads per
- * atom in the pair loop (power of two <= 32); cluster: CTAs per replica
- * (thread-block cluster) used for speculative iterations.  Results do not
- * depend on the launch shape. */
+ * atom in the force gather (power of two <= 32); cluster: CTAs per replica
+ * (thread-block cluster) serving speculative iterations; warp_walkers: 0 =
+ * one walker per CTA, 1 = one walker per warp (threads/32 walkers per CTA).
+ * Results do not depend on the launch shape. */
 typedef struct JrLaunchConfig {
   int32_t threads;
   int32_t tpa;
   int32_t cluster;
+  int32_t warp_walkers;
 } JrLaunchConfig;
 
 /* ---- NS iterations (replaces the jit'd ns_step) ---- */

@@ -124,7 +124,8 @@ class JrInfoBuffers(C.Structure):
 
 
 class JrLaunchConfig(C.Structure):
-    _fields_ = [("threads", C.c_int32), ("tpa", C.c_int32), ("cluster", C.c_int32)]
+    _fields_ = [("threads", C.c_int32), ("tpa", C.c_int32), ("cluster", C.c_int32),
+                ("warp_walkers", C.c_int32)]
 
 
 #: Every symbol ``include/jaxrens_b200.h`` declares.

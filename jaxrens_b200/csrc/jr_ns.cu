@@ -1,18 +1,20 @@
 // jr_ns.cu -- B200 kernels and the C-ABI of the nested-sampling walk.
 //
 // Kernels
-//   ns_iterate_kernel  n_iter NS iterations for every replica in one launch.
-//                      A thread-block cluster of C CTAs serves one replica.
-//                      Each round predicts the culls of the next D iterations
-//                      (the PRNG stream is state independent, and the culled
-//                      walker of iteration i+d is the (d+1)-th highest energy
-//                      as long as the walkers written by iterations < d stay
-//                      below it), walks them concurrently, then commits the
-//                      longest prefix whose predictions hold.  Committed
-//                      results are exactly those of sequential ns_step calls.
-//   move_trial_kernel  one move on many walkers (adaptation trials, burn-in)
-//   energy_kernel      energy + forces of a batch of configurations
-//   re_swap_kernel     pressure / semi-grand replica-exchange pass
+//   ns_iterate_kernel<G>  n_iter NS iterations for every replica in one
+//                      launch.  A thread-block cluster of C CTAs serves one
+//                      replica; each CTA walks one chain (G = CtaGroup) or one
+//                      chain per warp (G = WarpGroup).  Each round predicts
+//                      the culls of the next D iterations -- the PRNG stream
+//                      is state independent, and the walker culled at
+//                      iteration i+d is the (d+1)-th highest energy as long as
+//                      the walkers written by iterations < d stay below it --
+//                      walks them concurrently, then commits the longest
+//                      prefix whose predictions hold.  Committed results are
+//                      exactly those of sequential ns_step calls.
+//   move_trial_kernel<G>  one move on many walkers (adaptation, burn-in)
+//   energy_kernel<G>      energy + forces of a batch of configurations
+//   re_swap_kernel        pressure / semi-grand replica-exchange pass
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -22,6 +24,7 @@
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <type_traits>
 
 #include "../../include/jaxrens_b200.h"
 #include "jr_rng.cuh"
@@ -31,8 +34,8 @@ namespace cg = cooperative_groups;
 
 namespace jr {
 
-constexpr int kMaxD = 16;          // speculative iterations per round
-constexpr int kMaxWalk = 256;      // D * (1 + n_extra) bound
+constexpr int kMaxD = 32;     // speculative iterations per round
+constexpr int kMaxWalk = 256; // D * (1 + n_extra) bound
 
 struct NsShared {
   int worst[kMaxD];
@@ -44,7 +47,7 @@ struct NsShared {
   int extras[kMaxWalk];
   int wset[kMaxWalk];
   int n_wset;
-  double res_E;                    // final energy of this CTA's chain
+  double res_E[kMaxWarps];  // final energy of each chain this CTA walked
   unsigned long long u64[2][kMaxWarps];
   int flag[2][kMaxWarps];
 };
@@ -59,8 +62,7 @@ __device__ __forceinline__ double unord_double(unsigned long long k) {
 }
 
 // Block max of a u64 and OR of an int flag; uniform result in every thread.
-__device__ inline void block_max_u64(NsShared& ns, int& par, unsigned long long& v,
-                                     int& f) {
+__device__ inline void block_max_u64(NsShared& ns, int& par, unsigned long long& v, int& f) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nw = (blockDim.x + 31) >> 5;
   for (int off = 16; off > 0; off >>= 1) {
@@ -90,10 +92,9 @@ __device__ __forceinline__ bool in_set(const int* set, int n, int k) {
 
 // _find_worst_walker (nested_sampling.py:86-109) over the candidates not in
 // `excl`: jnp.max (NaN-propagating), then argmax of uniform noise among the
-// exact ties (first index on equal noise).
-__device__ void cull_select(NsShared& ns, int& par, const double* E, int K,
-                            const int* excl, int nexcl, Key kworst, int& worst,
-                            double& emax, bool& any_nan) {
+// exact ties (first index on equal noise).  CTA-wide.
+__device__ void cull_select(NsShared& ns, int& par, const double* E, int K, const int* excl,
+                            int nexcl, Key kworst, int& worst, double& emax, bool& any_nan) {
   unsigned long long best = 0;
   int nanf = 0;
   for (int k = threadIdx.x; k < K; k += blockDim.x) {
@@ -131,9 +132,8 @@ __device__ void cull_select(NsShared& ns, int& par, const double* E, int K,
 
 // _get_extra_indices (nested_sampling.py:112-133): the n_extra largest uniform
 // noises, worst and clone excluded, stable (lower index first on ties).
-__device__ void select_extras(NsShared& ns, int& par, float* noise, int K,
-                              int worst, int clone, Key kextra, int n_extra,
-                              int* out) {
+__device__ void select_extras(NsShared& ns, int& par, float* noise, int K, int worst, int clone,
+                              Key kextra, int n_extra, int* out) {
   for (int k = threadIdx.x; k < K; k += blockDim.x)
     noise[k] = (k == worst || k == clone) ? -1.0f : uniform01(bits32(kextra, (uint32_t)k));
   __syncthreads();
@@ -164,32 +164,31 @@ __device__ __forceinline__ double logaddexp(double a, double b) {
   return amax + log1p(exp(-fabs(delta)));
 }
 
-__device__ inline void walk_chain(const JrParams& P, Walker& w, int T, Key chain_key,
-                                  Key move_key, double emax, float pressure,
-                                  const float* mu) {
+template <class G>
+__device__ __forceinline__ void walk_chain(const JrParams& P, Walker<G>& w, int T, Key chain_key,
+                                  Key move_key, double emax, float pressure, const float* mu) {
   for (int t = 0; t < T; ++t)
-    mwg_step(P, w, split(chain_key, (uint32_t)t), split(move_key, (uint32_t)t), emax,
-             pressure, mu);
-  __syncthreads();
+    mwg_step(P, w, split(chain_key, (uint32_t)t), split(move_key, (uint32_t)t), emax, pressure,
+             mu);
+  w.g.sync();
 }
 
 // Copy the about-to-be-culled walker of replica p into info row `row`.
-__device__ inline void write_dead(const JrDims& D, const JrStateBuffers& st,
-                                  const JrInfoBuffers& info, int row, int p, int slot,
-                                  int n) {
+template <class G>
+__device__ inline void write_dead(const G& g, const JrDims& D, const JrStateBuffers& st,
+                                  const JrInfoBuffers& info, int row, int p, int slot, int n) {
   const int K = D.n_walkers, Nmax = D.n_atoms_max, Pn = D.n_replicas;
   const size_t wb = (size_t)p * K + slot;
   const size_t ib = (size_t)row * Pn + p;
+  const int r0 = g.rank(), gs = g.size();
   if (info.dead_positions)
-    for (int q = threadIdx.x; q < 3 * n; q += blockDim.x)
+    for (int q = r0; q < 3 * n; q += gs)
       info.dead_positions[ib * Nmax * 3 + q] = st.positions[wb * Nmax * 3 + q];
   if (info.dead_types)
-    for (int q = threadIdx.x; q < n; q += blockDim.x)
-      info.dead_types[ib * Nmax + q] = st.types[wb * Nmax + q];
+    for (int q = r0; q < n; q += gs) info.dead_types[ib * Nmax + q] = st.types[wb * Nmax + q];
   if (info.dead_cell)
-    for (int q = threadIdx.x; q < 9; q += blockDim.x)
-      info.dead_cell[ib * 9 + q] = st.cell[wb * 9 + q];
-  __syncthreads();
+    for (int q = r0; q < 9; q += gs) info.dead_cell[ib * 9 + q] = st.cell[wb * 9 + q];
+  g.sync();
 }
 
 __device__ inline void copy_params(JrParams& dst, const JrParams& src) {
@@ -199,29 +198,91 @@ __device__ inline void copy_params(JrParams& dst, const JrParams& src) {
   for (int q = threadIdx.x; q < nw; q += blockDim.x) d[q] = s[q];
 }
 
-__global__ void __launch_bounds__(512)
+// Dynamic smem of the NS kernel: [K doubles][K floats][pair table][walkers].
+struct DynLayout {
+  double* Epop;
+  float* noise;
+  uint16_t* pij;
+  char* walkers;
+  size_t walker_bytes;
+};
+
+__host__ __device__ inline size_t dyn_head_bytes(int K, int nmax, int nimg) {
+  return align16(8u * (size_t)K) + align16(4u * (size_t)K) + pair_table_bytes(nmax, nimg);
+}
+
+__device__ inline DynLayout dyn_layout(unsigned char* dyn, int K, int nmax, int nimg) {
+  DynLayout L;
+  char* p = reinterpret_cast<char*>(dyn);
+  L.Epop = reinterpret_cast<double*>(p);
+  p += align16(8u * (size_t)K);
+  L.noise = reinterpret_cast<float*>(p);
+  p += align16(4u * (size_t)K);
+  L.pij = use_pair_matrix(nmax, nimg) ? reinterpret_cast<uint16_t*>(p) : nullptr;
+  p += pair_table_bytes(nmax, nimg);
+  L.walkers = p;
+  L.walker_bytes = walker_smem_bytes(nmax, nimg);
+  return L;
+}
+
+template <class G>
+__device__ __forceinline__ G make_group(double (*red)[kMaxWarps][3]);
+template <>
+__device__ __forceinline__ CtaGroup make_group<CtaGroup>(double (*red)[kMaxWarps][3]) {
+  return CtaGroup{red};
+}
+template <>
+__device__ __forceinline__ WarpGroup make_group<WarpGroup>(double (*)[kMaxWarps][3]) {
+  return WarpGroup{};
+}
+
+// Pair decode table of one group's walker (the group's own n).
+template <class G>
+__device__ inline void build_group_pair_table(const G& g, uint16_t* pij, int n) {
+  if (!pij) return;
+  const int np = n * (n - 1) / 2;
+  for (int q = g.rank(); q < np; q += g.size()) {
+    int a = 0;
+    while ((a + 1) * (2 * n - a - 2) / 2 <= q) ++a;
+    pij[q] = (uint16_t)(a | ((q - a * (2 * n - a - 1) / 2 + a + 1) << 8));
+  }
+  g.sync();
+}
+
+template <class G, int kMaxThreads>
+__global__ void __launch_bounds__(kMaxThreads, 1)
 ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
-                  const JrInfoBuffers info, const int n_iter, const int tpa,
-                  const int C, const uint32_t* __restrict__ key0_base) {
+                  const JrInfoBuffers info, const int n_iter, const int tpa, const int C,
+                  const uint32_t* __restrict__ key0_base) {
+  constexpr bool kWarp = std::is_same<G, WarpGroup>::value;
   extern __shared__ __align__(16) unsigned char dyn[];
-  __shared__ WalkShared ws;
   __shared__ NsShared ns;
   __shared__ JrParams P;
+  __shared__ PairTables tab;
+  __shared__ double red[2][kMaxWarps][3];
   copy_params(P, Pg);
   cg::cluster_group cluster = cg::this_cluster();
   const int p = blockIdx.x / C;
   const int c = blockIdx.x % C;
   const int K = D.n_walkers, M = D.n_moves, T = D.n_mcmc_steps;
   const int nx = D.n_extra, W = 1 + nx;
-  const int n = st.n_atoms[p];
-  const int Dmax = (C >= 2 * W) ? (C / W < kMaxD ? C / W : kMaxD) : 1;
-  WalkArrays arr = carve(dyn, D.n_atoms_max, Pg.model.n_images);
-  double* Epop = reinterpret_cast<double*>(dyn + walk_dyn_smem_bytes(D.n_atoms_max, Pg.model.n_images));
-  float* noise = reinterpret_cast<float*>(Epop + K);
-  Walker w{ws, arr, n, tpa, 0};
+  const int n = min(max(st.n_atoms[p], 1), D.n_atoms_max);
+  const int nimg = Pg.model.n_images;
+  const int cpc = kWarp ? (int)(blockDim.x >> 5) : 1;  // chains per CTA
+  const int my = kWarp ? (int)(threadIdx.x >> 5) : 0;  // this group's chain in the CTA
+  const int slots = C * cpc;
+  const int s_my = c * cpc + my;
+  const int Dmax = (slots >= 2 * W) ? (slots / W < kMaxD ? slots / W : kMaxD) : 1;
+  DynLayout L = dyn_layout(dyn, K, D.n_atoms_max, nimg);
+  WalkArrays arr;
+  WalkShared* wsp = carve_walker(L.walkers + (size_t)my * L.walker_bytes, D.n_atoms_max, nimg,
+                                 L.pij, arr);
+  Walker<G> w{*wsp, arr, tab, n, tpa, make_group<G>(red), 0};
   int par = 0;
   __syncthreads();
-  load_tables(P, ws);
+  load_tables(P, tab);
+  build_pair_table(L.pij, n);
+  __syncthreads();
   const float pressure = st.pressure[p];
   const float* mu = st.mu ? st.mu + (size_t)p * P.model.n_species : nullptr;
   Key key{st.rng_key[2 * p], st.rng_key[2 * p + 1]};
@@ -231,7 +292,7 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
   int committed = 0, rounds = 0;
   while (committed < n_iter) {
     const int Dr = (n_iter - committed) < Dmax ? (n_iter - committed) : Dmax;
-    for (int k = threadIdx.x; k < K; k += blockDim.x) Epop[k] = st.energy64[(size_t)p * K + k];
+    for (int k = threadIdx.x; k < K; k += blockDim.x) L.Epop[k] = st.energy64[(size_t)p * K + k];
     if (threadIdx.x == 0) ns.n_wset = 0;
     __syncthreads();
     // ---- predictions for iterations d < Dr (every CTA, identically) ----
@@ -243,10 +304,10 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
       int worst;
       double emax;
       bool any_nan;
-      cull_select(ns, par, Epop, K, ns.wset, ns.n_wset, kw, worst, emax, any_nan);
+      cull_select(ns, par, L.Epop, K, ns.wset, ns.n_wset, kw, worst, emax, any_nan);
       int clone = randint(kclone, 0, K - 1);
       if (clone >= worst) clone += 1;
-      if (nx > 0) select_extras(ns, par, noise, K, worst, clone, kextra, nx, ns.extras + d * nx);
+      if (nx > 0) select_extras(ns, par, L.noise, K, worst, clone, kextra, nx, ns.extras + d * nx);
       __syncthreads();
       if (threadIdx.x == 0) {
         bool sp = (d == 0);
@@ -270,27 +331,28 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
       k0d = advance_iteration(k0d);
     }
     // ---- walk ----
-    zero_chain_counters(ws);
-    if (threadIdx.x == 0) ns.res_E = 0.0;
+    if (w.g.leader()) {
+      zero_chain_counters(w.s);
+      ns.res_E[my] = 0.0;
+    }
     __syncthreads();
     if (Dmax == 1) {
-      for (int sidx = c; sidx < W; sidx += C) {
+      for (int sidx = s_my; sidx < W; sidx += slots) {
         const int src = sidx == 0 ? ns.clone[0] : ns.extras[sidx - 1];
         const int dst = sidx == 0 ? ns.worst[0] : src;
-        if (sidx == 0) write_dead(D, st, info, committed, p, ns.worst[0], n);
+        if (sidx == 0) write_dead(w.g, D, st, info, committed, p, ns.worst[0], n);
         load_walker(P, D, st, w, p, src, sidx == 0);
-        walk_chain(P, w, T, split(ns.kmcmc[0], (uint32_t)sidx), ns.kmove[0], ns.e[0],
-                   pressure, mu);
+        walk_chain(P, w, T, split(ns.kmcmc[0], (uint32_t)sidx), ns.kmove[0], ns.e[0], pressure,
+                   mu);
         store_walker(D, st, w, p, dst);
       }
     } else {
-      const int d = c / W, wi = c % W;
+      const int d = s_my / W, wi = s_my % W;
       if (d < Dr && ns.spec[d]) {
         const int src = wi == 0 ? ns.clone[d] : ns.extras[d * nx + wi - 1];
         load_walker(P, D, st, w, p, src, wi == 0);
-        walk_chain(P, w, T, split(ns.kmcmc[d], (uint32_t)wi), ns.kmove[d], ns.e[d],
-                   pressure, mu);
-        if (threadIdx.x == 0) ns.res_E = ws.E;
+        walk_chain(P, w, T, split(ns.kmcmc[d], (uint32_t)wi), ns.kmove[d], ns.e[d], pressure, mu);
+        if (w.g.leader()) ns.res_E[my] = w.s.E;
       }
     }
     __syncthreads();
@@ -304,16 +366,17 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
         bool ok = ns.spec[d] != 0;
         for (int d2 = 0; d2 < d && ok; ++d2)
           for (int w2 = 0; w2 < W && ok; ++w2) {
-            const double* r = cluster.map_shared_rank(&ns.res_E, d2 * W + w2);
+            const int sl = d2 * W + w2;
+            const double* r = cluster.map_shared_rank(&ns.res_E[sl % cpc], sl / cpc);
             if (!(*r < ns.e[d])) ok = false;
           }
         if (!ok) break;
         ++nval;
       }
-      const int d = c / W, wi = c % W;
+      const int d = s_my / W, wi = s_my % W;
       if (d < nval) {
         const int dst = wi == 0 ? ns.worst[d] : ns.extras[d * nx + wi - 1];
-        if (wi == 0) write_dead(D, st, info, committed + d, p, ns.worst[d], n);
+        if (wi == 0) write_dead(w.g, D, st, info, committed + d, p, ns.worst[d], n);
         store_walker(D, st, w, p, dst);
       }
     }
@@ -322,12 +385,14 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
       int it = iter;
       for (int d = 0; d < nval; ++d, ++it) {
         const size_t ib = (size_t)(committed + d) * D.n_replicas + p;
-        const int r0 = Dmax == 1 ? 0 : d * W;
-        const int r1 = Dmax == 1 ? C : d * W + W;
+        const int s0 = Dmax == 1 ? 0 : d * W;
+        const int s1 = Dmax == 1 ? (slots < W ? slots : W) : d * W + W;
         for (int m = 0; m < M; ++m) {
           int a = 0, pr = 0, ne = 0, ng = 0, rr[4] = {0, 0, 0, 0};
-          for (int r = r0; r < r1; ++r) {
-            WalkShared* rs = cluster.map_shared_rank(&ws, r);
+          for (int sl = s0; sl < s1; ++sl) {
+            const WalkShared* local = reinterpret_cast<const WalkShared*>(
+                L.walkers + (size_t)(sl % cpc) * L.walker_bytes);
+            const WalkShared* rs = cluster.map_shared_rank(local, sl / cpc);
             a += rs->c_acc[m];
             pr += rs->c_prop[m];
             ne += rs->c_nev[m];
@@ -371,27 +436,49 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
 }
 
 // ------------------------------------------------------------ trials ----
-__global__ void __launch_bounds__(512)
-move_trial_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
-                  const int n_trials, const int move_idx, const int* walker_idx,
-                  const uint32_t* keys, const uint32_t* move_keys, const float* step,
-                  const double* emax, const int write_back, int* accepted,
-                  int* reject_reason, const int tpa) {
+// One walker per group; the grid covers P * n_trials walkers.  Walkers of one
+// CTA may belong to different replicas, so every group has its own pair table.
+template <class G, int kMaxThreads>
+__global__ void __launch_bounds__(kMaxThreads, 1)
+move_trial_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st, const int n_trials,
+                  const int move_idx, const int* walker_idx, const uint32_t* keys,
+                  const uint32_t* move_keys, const float* step, const double* emax,
+                  const int write_back, int* accepted, int* reject_reason, const int tpa) {
+  constexpr bool kWarp = std::is_same<G, WarpGroup>::value;
   extern __shared__ __align__(16) unsigned char dyn[];
-  __shared__ WalkShared ws;
   __shared__ JrParams P;
+  __shared__ PairTables tab;
+  __shared__ double red[2][kMaxWarps][3];
   copy_params(P, Pg);
-  const int p = blockIdx.x / n_trials;
-  const int t = blockIdx.x % n_trials;
-  const int n = st.n_atoms[p];
-  WalkArrays arr = carve(dyn, D.n_atoms_max, Pg.model.n_images);
-  Walker w{ws, arr, n, tpa, 0};
+  const int gpc = kWarp ? (int)(blockDim.x >> 5) : 1;
+  const int my = kWarp ? (int)(threadIdx.x >> 5) : 0;
+  const int total = D.n_replicas * n_trials;
+  const int t_global = blockIdx.x * gpc + my;
+  const int nimg = Pg.model.n_images;
+  const size_t ptb = pair_table_bytes(D.n_atoms_max, nimg);
+  char* base = reinterpret_cast<char*>(dyn) +
+               (size_t)my * (ptb + walker_smem_bytes(D.n_atoms_max, nimg));
+  uint16_t* pij = ptb ? reinterpret_cast<uint16_t*>(base) : nullptr;
+  WalkArrays arr;
+  WalkShared* wsp = carve_walker(base + ptb, D.n_atoms_max, nimg, pij, arr);
   __syncthreads();
-  load_tables(P, ws);
-  const size_t tb = (size_t)p * n_trials + t;
+  load_tables(P, tab);
+  __syncthreads();
+  if (t_global >= total) return;  // whole group leaves together
+  const int p = t_global / n_trials;
+  const int n = min(max(st.n_atoms[p], 1), D.n_atoms_max);
+  Walker<G> w{*wsp, arr, tab, n, tpa, make_group<G>(red), 0};
+  build_group_pair_table(w.g, pij, n);
+  const size_t tb = (size_t)t_global;
   const int slot = walker_idx[tb];
+  if (slot < 0 || slot >= D.n_walkers) {  // invalid index: report, touch nothing
+    if (w.g.leader()) {
+      accepted[tb] = -1;
+      if (reject_reason) reject_reason[tb] = -1;
+    }
+    return;
+  }
   load_walker(P, D, st, w, p, slot, false);
-  const float pressure = st.pressure[p];
   const float* mu = st.mu ? st.mu + (size_t)p * P.model.n_species : nullptr;
   const Key key{keys[2 * tb], keys[2 * tb + 1]};
   int idx = move_idx;
@@ -400,79 +487,95 @@ move_trial_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
     idx = choice(mk, P.moves.cum_probs, P.moves.n_moves);
   }
   int reason = 0;
-  const bool acc = run_move(P, w, idx, key, step[p], emax[p], pressure, mu, reason);
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  const bool acc = run_move(P, w, idx, key, step[p], emax[p], st.pressure[p], mu, reason);
+  w.g.sync();
+  if (w.g.leader()) {
     accepted[tb] = acc ? 1 : 0;
     if (reject_reason) reject_reason[tb] = acc ? 0 : (reason > 1 ? reason : 1);
     if (write_back) {
-      ws.w_prop[idx] += 1;
-      ws.w_acc[idx] += acc ? 1 : 0;
+      w.s.w_prop[idx] += 1;
+      w.s.w_acc[idx] += acc ? 1 : 0;
     }
   }
   if (write_back) store_walker(D, st, w, p, slot);
 }
 
 // ------------------------------------------------------------ energy ----
-__global__ void __launch_bounds__(512)
-energy_kernel(const JrParams Pg, const int nmax, const float* positions,
+template <class G, int kMaxThreads>
+__global__ void __launch_bounds__(kMaxThreads, 1)
+energy_kernel(const JrParams Pg, const int n_configs, const int nmax, const float* positions,
               const int32_t* types, const float* cell, const int32_t* n_atoms,
-              const float* pressure, const float* mu, double* energy64,
-              double* energy_u, float* forces, const int tpa) {
+              const float* pressure, const float* mu, double* energy64, double* energy_u,
+              float* forces, const int tpa) {
+  constexpr bool kWarp = std::is_same<G, WarpGroup>::value;
   extern __shared__ __align__(16) unsigned char dyn[];
-  __shared__ WalkShared ws;
   __shared__ JrParams P;
+  __shared__ PairTables tab;
+  __shared__ double red[2][kMaxWarps][3];
   copy_params(P, Pg);
-  const int b = blockIdx.x;
-  const int n = n_atoms[b];
-  WalkArrays arr = carve(dyn, nmax, Pg.model.n_images);
-  Walker w{ws, arr, n, tpa, 0};
+  const int gpc = kWarp ? (int)(blockDim.x >> 5) : 1;
+  const int my = kWarp ? (int)(threadIdx.x >> 5) : 0;
+  const int b = blockIdx.x * gpc + my;
+  const int nimg = Pg.model.n_images;
+  const size_t ptb = pair_table_bytes(nmax, nimg);
+  char* base = reinterpret_cast<char*>(dyn) + (size_t)my * (ptb + walker_smem_bytes(nmax, nimg));
+  uint16_t* pij = ptb ? reinterpret_cast<uint16_t*>(base) : nullptr;
+  WalkArrays arr;
+  WalkShared* wsp = carve_walker(base + ptb, nmax, nimg, pij, arr);
   __syncthreads();
-  load_tables(P, ws);
-  for (int q = threadIdx.x; q < 3 * n; q += blockDim.x) {
+  load_tables(P, tab);
+  __syncthreads();
+  if (b >= n_configs) return;
+  const int n = min(max(n_atoms[b], 1), nmax);
+  const int smax = Pg.model.n_species - 1;
+  Walker<G> w{*wsp, arr, tab, n, tpa, make_group<G>(red), 0};
+  build_group_pair_table(w.g, pij, n);
+  const int r0 = w.g.rank(), gs = w.g.size();
+  for (int q = r0; q < 3 * n; q += gs) {
     pos_at(arr.xs, q) = positions[(size_t)b * nmax * 3 + q];
     arr.dir[q] = 0.0f;
   }
-  for (int i = threadIdx.x; i < n; i += blockDim.x)
-    arr.xs[i].w = __int_as_float(types[(size_t)b * nmax + i]);
-  if (threadIdx.x == 0) {
-    for (int q = 0; q < JR_MAX_SPECIES; ++q) ws.counts[q] = 0;
-    ws.cur = 0;
-    make_cell_ctx(cell + (size_t)b * 9, ws.cc[0], arr.T, P.model);
+  for (int i = r0; i < n; i += gs) {
+    const int t = types[(size_t)b * nmax + i];
+    arr.xs[i].w = __int_as_float(t < 0 ? 0 : (t > smax ? smax : t));
   }
-  __syncthreads();
-  if (threadIdx.x == 0)
-    for (int i = 0; i < n; ++i) ws.counts[__float_as_int(arr.xs[i].w)] += 1;
-  __syncthreads();
+  w.g.sync();
+  if (w.g.leader()) {
+    for (int q = 0; q < JR_MAX_SPECIES; ++q) w.s.counts[q] = 0;
+    for (int i = 0; i < n; ++i) w.s.counts[__float_as_int(arr.xs[i].w)] += 1;
+    w.s.cur = 0;
+    make_cell_ctx(cell + (size_t)b * 9, w.s.cc[0], arr.T, P.model);
+  }
+  w.g.sync();
   double U, sff, sfd;
   model_eval<true>(P, w, 0, U, sff, sfd);
   const float* m = mu ? mu + (size_t)b * P.model.n_species : nullptr;
   double E = U;
   if (P.model.model != JR_MODEL_GAUSS_MIX)
-    E = U + ensemble_term(ws, ws.cc[0].vol, pressure[b], m, P.model.n_species);
-  __syncthreads();
-  if (threadIdx.x == 0) {
+    E = U + ensemble_term(w.s, w.s.cc[0].vol, pressure[b], m, P.model.n_species);
+  w.g.sync();
+  if (w.g.leader()) {
     energy64[b] = E;
     if (energy_u) energy_u[b] = U;
   }
   if (forces)
-    for (int q = threadIdx.x; q < 3 * n; q += blockDim.x)
-      forces[(size_t)b * nmax * 3 + q] = arr.F[q];
+    for (int q = r0; q < 3 * n; q += gs) forces[(size_t)b * nmax * 3 + q] = arr.F[q];
 }
 
 // --------------------------------------------------------- RE swaps ----
-__device__ double walker_ens(const JrDims& D, const JrStateBuffers& st, int p, int slot,
-                             int S) {
+// Ensemble term of walker (p_conf, slot) under replica p_ens's parameters.
+__device__ double walker_ens(const JrDims& D, const JrStateBuffers& st, int p_conf, int slot,
+                             int p_ens, int S) {
   const int K = D.n_walkers, Nmax = D.n_atoms_max;
-  const size_t wb = (size_t)p * K + slot;
+  const size_t wb = (size_t)p_conf * K + slot;
   const float vol = fabsf(det3(st.cell + wb * 9));
-  double e = (double)st.pressure[p] * (double)vol;
+  double e = (double)st.pressure[p_ens] * (double)vol;
   if (st.mu) {
     int counts[JR_MAX_SPECIES] = {0};
-    const int n = st.n_atoms[p];
-    for (int i = 0; i < n; ++i) counts[st.types[wb * Nmax + i]]++;
+    const int n = min(max(st.n_atoms[p_conf], 1), Nmax);
+    for (int i = 0; i < n; ++i) counts[min(max(st.types[wb * Nmax + i], 0), S - 1)]++;
     double dot = 0.0;
-    for (int q = 0; q < S; ++q) dot += (double)st.mu[(size_t)p * S + q] * (double)counts[q];
+    for (int q = 0; q < S; ++q) dot += (double)st.mu[(size_t)p_ens * S + q] * (double)counts[q];
     e = e - dot;
   }
   return e;
@@ -489,8 +592,7 @@ __device__ void swap_range(Tp* a, Tp* b, int n) {
 
 // replica_exchange_step with EnsembleSwap (replica_exchange.py:318-436).
 __global__ void re_swap_kernel(const JrDims D, const JrStateBuffers st, const Key key,
-                               const int n_cycles, const int S, int* acc_pp,
-                               int* att_pp) {
+                               const int n_cycles, const int S, int* acc_pp, int* att_pp) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int R = D.n_replicas, K = D.n_walkers, Nmax = D.n_atoms_max;
   const int n_even = R / 2, n_odd = (R - 1) / 2;
@@ -511,37 +613,11 @@ __global__ void re_swap_kernel(const JrDims D, const JrStateBuffers st, const Ke
         if (slot >= nv) continue;
         const int ri = phase + 2 * slot, rj = ri + 1;
         const size_t bi = (size_t)ri * K + wi, bj = (size_t)rj * K + wj;
-        const double into_i = (st.energy64[bj] - walker_ens(D, st, rj, wj, S)) +
-                              [&] {
-                                // walker j's configuration in run i's ensemble
-                                const float vol = fabsf(det3(st.cell + bj * 9));
-                                double e = (double)st.pressure[ri] * (double)vol;
-                                if (st.mu) {
-                                  int cnt[JR_MAX_SPECIES] = {0};
-                                  for (int a = 0; a < st.n_atoms[rj]; ++a)
-                                    cnt[st.types[bj * Nmax + a]]++;
-                                  double dot = 0.0;
-                                  for (int q = 0; q < S; ++q)
-                                    dot += (double)st.mu[(size_t)ri * S + q] * (double)cnt[q];
-                                  e = e - dot;
-                                }
-                                return e;
-                              }();
-        const double into_j = (st.energy64[bi] - walker_ens(D, st, ri, wi, S)) +
-                              [&] {
-                                const float vol = fabsf(det3(st.cell + bi * 9));
-                                double e = (double)st.pressure[rj] * (double)vol;
-                                if (st.mu) {
-                                  int cnt[JR_MAX_SPECIES] = {0};
-                                  for (int a = 0; a < st.n_atoms[ri]; ++a)
-                                    cnt[st.types[bi * Nmax + a]]++;
-                                  double dot = 0.0;
-                                  for (int q = 0; q < S; ++q)
-                                    dot += (double)st.mu[(size_t)rj * S + q] * (double)cnt[q];
-                                  e = e - dot;
-                                }
-                                return e;
-                              }();
+        // into_i: walker j re-expressed in run i's ensemble (ensemble.py:62-87)
+        const double into_i =
+            (st.energy64[bj] - walker_ens(D, st, rj, wj, rj, S)) + walker_ens(D, st, rj, wj, ri, S);
+        const double into_j =
+            (st.energy64[bi] - walker_ens(D, st, ri, wi, ri, S)) + walker_ens(D, st, ri, wi, rj, S);
         const bool do_swap = (into_i < st.emax[ri]) && (into_j < st.emax[rj]);
         if (do_swap) {
           swap_range(st.positions + bi * Nmax * 3, st.positions + bj * Nmax * 3, Nmax * 3);
@@ -558,6 +634,24 @@ __global__ void re_swap_kernel(const JrDims D, const JrStateBuffers st, const Ke
       }
     }
   }
+}
+
+// Independent FMA chains per thread: the FP32 FMA pipe's attainable rate.
+__global__ void __launch_bounds__(256) fma_peak_kernel(float* out, int iters) {
+  float a0 = threadIdx.x * 1e-7f, a1 = a0 + 1e-7f, a2 = a0 + 2e-7f, a3 = a0 + 3e-7f;
+  float a4 = a0 + 4e-7f, a5 = a0 + 5e-7f, a6 = a0 + 6e-7f, a7 = a0 + 7e-7f;
+  const float b = 0.999999f, c = 1e-7f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      a0 = __fmaf_rn(a0, b, c); a1 = __fmaf_rn(a1, b, c);
+      a2 = __fmaf_rn(a2, b, c); a3 = __fmaf_rn(a3, b, c);
+      a4 = __fmaf_rn(a4, b, c); a5 = __fmaf_rn(a5, b, c);
+      a6 = __fmaf_rn(a6, b, c); a7 = __fmaf_rn(a7, b, c);
+    }
+  }
+  const float s = ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
+  if (s == 12345.678f) out[blockIdx.x] = s;  // keeps the chains live
 }
 
 }  // namespace jr
@@ -588,9 +682,8 @@ std::mutex g_tune_mu;
 std::map<TuneKey, JrLaunchConfig> g_tune_cache;
 
 TuneKey tune_key(const JrDims* d, const JrParams* p) {
-  return TuneKey{d->n_replicas, d->n_walkers, d->n_atoms_max, d->n_moves,
-                 d->n_mcmc_steps, d->n_extra, p->model.n_species, p->model.n_images,
-                 p->model.model};
+  return TuneKey{d->n_replicas, d->n_walkers, d->n_atoms_max, d->n_moves, d->n_mcmc_steps,
+                 d->n_extra, p->model.n_species, p->model.n_images, p->model.model};
 }
 
 int pow2_floor(int x) {
@@ -599,16 +692,27 @@ int pow2_floor(int x) {
   return p;
 }
 
+int warp_tpa(int nmax) {
+  int t = pow2_floor(32 / (nmax > 0 ? nmax : 1));
+  return t < 1 ? 1 : t;
+}
+
+// Small walkers: one warp per walker, four walkers per CTA, one CTA per
+// replica; larger walkers: one CTA per walker.
 JrLaunchConfig heuristic_config(const JrDims* d) {
   JrLaunchConfig c;
   const int nmax = d->n_atoms_max;
-  c.threads = nmax <= 48 ? 256 : 512;
-  // as many threads per atom as the CTA allows, capped at 8
-  int tpa = pow2_floor(c.threads / (nmax > 0 ? nmax : 1));
-  if (tpa > 8) tpa = 8;
-  if (tpa < 1) tpa = 1;
-  c.tpa = tpa;
   c.cluster = 1;
+  if (nmax <= 64) {
+    c.warp_walkers = 1;
+    c.threads = 128;
+    c.tpa = warp_tpa(nmax);
+  } else {
+    c.warp_walkers = 0;
+    c.threads = 512;
+    int tpa = pow2_floor(c.threads / nmax);
+    c.tpa = tpa > 16 ? 16 : (tpa < 1 ? 1 : tpa);
+  }
   return c;
 }
 
@@ -620,10 +724,8 @@ int check_params(const JrDims* d, const JrParams* p) {
                                   std::to_string(JR_MAX_ATOMS));
   if (d->n_moves < 1 || d->n_moves > JR_MAX_MOVES || d->n_moves != p->moves.n_moves)
     return fail(JR_ERR_SHAPE, "n_moves must be in [1, 8] and match params.moves");
-  if (d->n_cull != 1)
-    return fail(JR_ERR_UNSUPPORTED, "this build implements n_cull == 1 only");
-  if (d->n_extra < 0 || d->n_extra > d->n_walkers - 2 ||
-      d->n_extra + 1 > jr::kMaxWalk)
+  if (d->n_cull != 1) return fail(JR_ERR_UNSUPPORTED, "this build implements n_cull == 1 only");
+  if (d->n_extra < 0 || d->n_extra > d->n_walkers - 2 || d->n_extra + 1 > jr::kMaxWalk)
     return fail(JR_ERR_SHAPE, "n_extra must satisfy 0 <= n_extra <= n_walkers-2 and <= 255");
   if (p->model.n_species < 1 || p->model.n_species > JR_MAX_SPECIES)
     return fail(JR_ERR_PARAM, "n_species must be in [1, 8]");
@@ -645,64 +747,42 @@ int check_config(const JrLaunchConfig& c, const JrDims* d) {
     return fail(JR_ERR_PARAM, "threads must be a multiple of 32 in [32, 512]");
   if (c.tpa < 1 || c.tpa > 32 || (c.tpa & (c.tpa - 1)))
     return fail(JR_ERR_PARAM, "tpa must be a power of two <= 32");
-  if (c.cluster < 1 || c.cluster > 16)
-    return fail(JR_ERR_PARAM, "cluster must be in [1, 16]");
+  if (c.cluster < 1 || c.cluster > 16) return fail(JR_ERR_PARAM, "cluster must be in [1, 16]");
+  if (c.warp_walkers != 0 && c.warp_walkers != 1)
+    return fail(JR_ERR_PARAM, "warp_walkers must be 0 or 1");
+  if (!c.warp_walkers && c.tpa > c.threads) return fail(JR_ERR_PARAM, "tpa exceeds the CTA");
+  if (c.warp_walkers && c.threads > 128)
+    return fail(JR_ERR_PARAM, "warp-walker CTAs hold at most 4 walkers (128 threads)");
   const int W = 1 + d->n_extra;
-  if (c.cluster >= 2 * W && (c.cluster / W) * d->n_extra > jr::kMaxWalk)
-    return fail(JR_ERR_PARAM, "cluster * n_extra too large for speculation");
+  const int slots = c.cluster * (c.warp_walkers ? c.threads / 32 : 1);
+  if (slots >= 2 * W) {
+    const int D = slots / W < jr::kMaxD ? slots / W : jr::kMaxD;
+    if (D * d->n_extra > jr::kMaxWalk || D * W > jr::kMaxWalk)
+      return fail(JR_ERR_PARAM, "speculation depth * n_extra too large");
+  }
   return JR_OK;
 }
 
-size_t ns_dyn_smem(const JrDims* d, const JrParams* p) {
-  return jr::walk_dyn_smem_bytes(d->n_atoms_max, p->model.n_images) +
-         (size_t)d->n_walkers * (sizeof(double) + sizeof(float));
+size_t ns_dyn_smem(const JrDims* d, const JrParams* p, const JrLaunchConfig& c) {
+  const int cpc = c.warp_walkers ? c.threads / 32 : 1;
+  return jr::dyn_head_bytes(d->n_walkers, d->n_atoms_max, p->model.n_images) +
+         (size_t)cpc * jr::walker_smem_bytes(d->n_atoms_max, p->model.n_images);
 }
 
-}  // namespace
-
-extern "C" {
-
-const char* jr_last_error(void) { return g_last_error.c_str(); }
-
-int jr_version(void) { return 1; }
-
-size_t jr_ns_iterate_workspace_size(const JrDims* dims) {
-  (void)dims;
-  return 256;
+size_t group_dyn_smem(int nmax, int nimg, int groups) {
+  return (size_t)groups * (jr::pair_table_bytes(nmax, nimg) + jr::walker_smem_bytes(nmax, nimg));
 }
 
-int jr_ns_iterate(const JrDims* dims, const JrParams* params,
-                  const JrStateBuffers* state, const JrInfoBuffers* info,
-                  int32_t n_iter, const JrLaunchConfig* cfg, void* workspace,
-                  size_t workspace_bytes, void* stream) {
-  int rc = check_params(dims, params);
-  if (rc) return rc;
-  if (!state) return fail(JR_ERR_PARAM, "null state");
-  if (n_iter < 1) return fail(JR_ERR_PARAM, "n_iter must be >= 1");
-  if (!workspace || workspace_bytes < jr_ns_iterate_workspace_size(dims))
-    return fail(JR_ERR_WORKSPACE, "workspace missing or smaller than jr_ns_iterate_workspace_size()");
-  JrLaunchConfig c;
-  if (cfg) {
-    c = *cfg;
-  } else {
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tune_cache.find(tune_key(dims, params));
-    c = it != g_tune_cache.end() ? it->second : heuristic_config(dims);
-  }
-  rc = check_config(c, dims);
-  if (rc) return rc;
-  JrInfoBuffers inf{};
-  if (info) inf = *info;
-  cudaStream_t s = (cudaStream_t)stream;
-  cudaError_t e = cudaMemcpyAsync(workspace, state->rng_key, 2 * sizeof(uint32_t),
-                                  cudaMemcpyDeviceToDevice, s);
-  if (e != cudaSuccess) return cuda_fail(e, "key snapshot");
-  const size_t smem = ns_dyn_smem(dims, params);
-  e = cudaFuncSetAttribute(jr::ns_iterate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
+template <class G>
+int launch_ns(const JrDims* dims, const JrParams* params, const JrStateBuffers* state,
+              const JrInfoBuffers& inf, int n_iter, const JrLaunchConfig& c, void* workspace,
+              cudaStream_t s) {
+  const size_t smem = ns_dyn_smem(dims, params, c);
+  cudaError_t e = cudaFuncSetAttribute(jr::ns_iterate_kernel<G, std::is_same<G, jr::WarpGroup>::value ? 128 : 512>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "smem attribute");
   if (c.cluster > 8) {
-    e = cudaFuncSetAttribute(jr::ns_iterate_kernel,
+    e = cudaFuncSetAttribute(jr::ns_iterate_kernel<G, std::is_same<G, jr::WarpGroup>::value ? 128 : 512>,
                              cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e != cudaSuccess) return cuda_fail(e, "non-portable cluster attribute");
   }
@@ -718,34 +798,91 @@ int jr_ns_iterate(const JrDims* dims, const JrParams* params,
   attr[0].val.clusterDim.z = 1;
   lc.attrs = attr;
   lc.numAttrs = 1;
-  e = cudaLaunchKernelEx(&lc, jr::ns_iterate_kernel, *dims, *params, *state, inf,
-                         (int)n_iter, (int)c.tpa, (int)c.cluster,
-                         (const uint32_t*)workspace);
+  e = cudaLaunchKernelEx(&lc, jr::ns_iterate_kernel<G, std::is_same<G, jr::WarpGroup>::value ? 128 : 512>, *dims, *params, *state, inf, n_iter,
+                         (int)c.tpa, (int)c.cluster, (const uint32_t*)workspace);
   if (e != cudaSuccess) return cuda_fail(e, "ns_iterate launch");
   return JR_OK;
 }
 
-int jr_move_trial(const JrDims* dims, const JrParams* params,
-                  const JrStateBuffers* state, int32_t n_trials, int32_t move_idx,
-                  const int32_t* walker_idx, const uint32_t* keys,
-                  const uint32_t* move_keys, const float* step, const double* emax,
-                  int32_t write_back, int32_t* accepted, int32_t* reject_reason,
-                  void* stream) {
+}  // namespace
+
+extern "C" {
+
+const char* jr_last_error(void) { return g_last_error.c_str(); }
+
+int jr_version(void) { return 2; }
+
+size_t jr_ns_iterate_workspace_size(const JrDims* dims) {
+  (void)dims;
+  return 256;
+}
+
+int jr_ns_iterate(const JrDims* dims, const JrParams* params, const JrStateBuffers* state,
+                  const JrInfoBuffers* info, int32_t n_iter, const JrLaunchConfig* cfg,
+                  void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = check_params(dims, params);
+  if (rc) return rc;
+  if (!state) return fail(JR_ERR_PARAM, "null state");
+  if (n_iter < 1) return fail(JR_ERR_PARAM, "n_iter must be >= 1");
+  if (!workspace || workspace_bytes < jr_ns_iterate_workspace_size(dims))
+    return fail(JR_ERR_WORKSPACE,
+                "workspace missing or smaller than jr_ns_iterate_workspace_size()");
+  JrLaunchConfig c;
+  if (cfg) {
+    c = *cfg;
+  } else {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(tune_key(dims, params));
+    c = it != g_tune_cache.end() ? it->second : heuristic_config(dims);
+  }
+  rc = check_config(c, dims);
+  if (rc) return rc;
+  JrInfoBuffers inf{};
+  if (info) inf = *info;
+  cudaStream_t s = (cudaStream_t)stream;
+  // snapshot of replica 0's key: the shared move schedule of every replica
+  cudaError_t e = cudaMemcpyAsync(workspace, state->rng_key, 2 * sizeof(uint32_t),
+                                  cudaMemcpyDeviceToDevice, s);
+  if (e != cudaSuccess) return cuda_fail(e, "key snapshot");
+  if (c.warp_walkers)
+    return launch_ns<jr::WarpGroup>(dims, params, state, inf, n_iter, c, workspace, s);
+  return launch_ns<jr::CtaGroup>(dims, params, state, inf, n_iter, c, workspace, s);
+}
+
+int jr_move_trial(const JrDims* dims, const JrParams* params, const JrStateBuffers* state,
+                  int32_t n_trials, int32_t move_idx, const int32_t* walker_idx,
+                  const uint32_t* keys, const uint32_t* move_keys, const float* step,
+                  const double* emax, int32_t write_back, int32_t* accepted,
+                  int32_t* reject_reason, void* stream) {
   int rc = check_params(dims, params);
   if (rc) return rc;
   if (n_trials < 1 || !walker_idx || !keys || !step || !emax || !accepted)
     return fail(JR_ERR_PARAM, "trial buffers missing or n_trials < 1");
   if (move_idx >= dims->n_moves) return fail(JR_ERR_PARAM, "move_idx out of range");
   if (move_idx < 0 && !move_keys) return fail(JR_ERR_PARAM, "move_keys needed when move_idx < 0");
-  JrLaunchConfig c = heuristic_config(dims);
-  const size_t smem = jr::walk_dyn_smem_bytes(dims->n_atoms_max, params->model.n_images);
+  const JrLaunchConfig c = heuristic_config(dims);
+  const int nimg = params->model.n_images;
+  const int total = dims->n_replicas * n_trials;
   cudaStream_t s = (cudaStream_t)stream;
-  cudaError_t e = cudaFuncSetAttribute(jr::move_trial_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return cuda_fail(e, "smem attribute");
-  jr::move_trial_kernel<<<dims->n_replicas * n_trials, c.threads, smem, s>>>(
-      *dims, *params, *state, n_trials, move_idx, walker_idx, keys, move_keys, step, emax,
-      write_back, accepted, reject_reason, c.tpa);
+  cudaError_t e;
+  if (c.warp_walkers) {
+    const int gpc = c.threads / 32;
+    const size_t smem = group_dyn_smem(dims->n_atoms_max, nimg, gpc);
+    e = cudaFuncSetAttribute(jr::move_trial_kernel<jr::WarpGroup, 128>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "smem attribute");
+    jr::move_trial_kernel<jr::WarpGroup, 128><<<(total + gpc - 1) / gpc, c.threads, smem, s>>>(
+        *dims, *params, *state, n_trials, move_idx, walker_idx, keys, move_keys, step, emax,
+        write_back, accepted, reject_reason, c.tpa);
+  } else {
+    const size_t smem = group_dyn_smem(dims->n_atoms_max, nimg, 1);
+    e = cudaFuncSetAttribute(jr::move_trial_kernel<jr::CtaGroup, 512>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "smem attribute");
+    jr::move_trial_kernel<jr::CtaGroup, 512><<<total, c.threads, smem, s>>>(
+        *dims, *params, *state, n_trials, move_idx, walker_idx, keys, move_keys, step, emax,
+        write_back, accepted, reject_reason, c.tpa);
+  }
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "move_trial launch");
   return JR_OK;
@@ -755,40 +892,63 @@ int jr_energy_forces(const JrParams* params, int32_t n_configs, int32_t n_atoms_
                      const float* positions, const int32_t* types, const float* cell,
                      const int32_t* n_atoms, const float* pressure, const float* mu,
                      double* energy64, double* energy_u, float* forces, void* stream) {
-  if (!params || n_configs < 1 || n_atoms_max < 1 || n_atoms_max > JR_MAX_ATOMS ||
-      !positions || !types || !cell || !n_atoms || !pressure || !energy64)
+  if (!params || n_configs < 1 || n_atoms_max < 1 || n_atoms_max > JR_MAX_ATOMS || !positions ||
+      !types || !cell || !n_atoms || !pressure || !energy64)
     return fail(JR_ERR_PARAM, "invalid energy_forces arguments");
   if (params->model.n_species < 1 || params->model.n_species > JR_MAX_SPECIES ||
       params->model.n_images < 1 || params->model.n_images > JR_MAX_IMAGES)
     return fail(JR_ERR_PARAM, "invalid model parameters");
   JrDims d{};
   d.n_atoms_max = n_atoms_max;
-  JrLaunchConfig c = heuristic_config(&d);
-  const size_t smem = jr::walk_dyn_smem_bytes(n_atoms_max, params->model.n_images);
+  const JrLaunchConfig c = heuristic_config(&d);
+  const int nimg = params->model.n_images;
   cudaStream_t s = (cudaStream_t)stream;
-  cudaError_t e = cudaFuncSetAttribute(jr::energy_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return cuda_fail(e, "smem attribute");
-  jr::energy_kernel<<<n_configs, c.threads, smem, s>>>(*params, n_atoms_max, positions, types,
-                                                      cell, n_atoms, pressure, mu, energy64,
-                                                      energy_u, forces, c.tpa);
+  cudaError_t e;
+  if (c.warp_walkers) {
+    const int gpc = c.threads / 32;
+    const size_t smem = group_dyn_smem(n_atoms_max, nimg, gpc);
+    e = cudaFuncSetAttribute(jr::energy_kernel<jr::WarpGroup, 128>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "smem attribute");
+    jr::energy_kernel<jr::WarpGroup, 128><<<(n_configs + gpc - 1) / gpc, c.threads, smem, s>>>(
+        *params, n_configs, n_atoms_max, positions, types, cell, n_atoms, pressure, mu, energy64,
+        energy_u, forces, c.tpa);
+  } else {
+    const size_t smem = group_dyn_smem(n_atoms_max, nimg, 1);
+    e = cudaFuncSetAttribute(jr::energy_kernel<jr::CtaGroup, 512>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "smem attribute");
+    jr::energy_kernel<jr::CtaGroup, 512><<<n_configs, c.threads, smem, s>>>(
+        *params, n_configs, n_atoms_max, positions, types, cell, n_atoms, pressure, mu, energy64,
+        energy_u, forces, c.tpa);
+  }
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "energy launch");
   return JR_OK;
 }
 
-int jr_re_swap(const JrDims* dims, const JrStateBuffers* state, uint32_t key0,
-               uint32_t key1, int32_t n_swap_cycles, int32_t n_species,
-               int32_t* acc_per_pair, int32_t* att_per_pair, void* stream) {
+int jr_re_swap(const JrDims* dims, const JrStateBuffers* state, uint32_t key0, uint32_t key1,
+               int32_t n_swap_cycles, int32_t n_species, int32_t* acc_per_pair,
+               int32_t* att_per_pair, void* stream) {
   if (!dims || !state) return fail(JR_ERR_PARAM, "null dims or state");
   if (n_swap_cycles < 0 || n_species < 1 || n_species > JR_MAX_SPECIES)
     return fail(JR_ERR_PARAM, "invalid swap parameters");
   if (dims->n_replicas < 2) return JR_OK;
-  jr::re_swap_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(
-      *dims, *state, jr::Key{key0, key1}, n_swap_cycles, n_species, acc_per_pair,
-      att_per_pair);
+  jr::re_swap_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(*dims, *state, jr::Key{key0, key1},
+                                                        n_swap_cycles, n_species, acc_per_pair,
+                                                        att_per_pair);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "re_swap launch");
+  return JR_OK;
+}
+
+int jr_bench_fma_peak(int n_blocks, int iters, float* scratch, double* flops, void* stream) {
+  if (n_blocks < 1 || iters < 1 || !scratch || !flops)
+    return fail(JR_ERR_PARAM, "fma_peak arguments");
+  jr::fma_peak_kernel<<<n_blocks, 256, 0, (cudaStream_t)stream>>>(scratch, iters);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "fma_peak launch");
+  *flops = 2.0 * 8.0 * 16.0 * (double)iters * 256.0 * (double)n_blocks;
   return JR_OK;
 }
 
@@ -814,8 +974,7 @@ struct ScratchState {
 
 // Scratch copy of the mutable state so candidate launch shapes can be timed
 // without touching the caller's walkers.  Freed before jr_autotune returns.
-int clone_state(const JrDims* d, const JrParams* p, const JrStateBuffers* s,
-                ScratchState& out, cudaStream_t st) {
+int clone_state(const JrDims* d, const JrStateBuffers* s, ScratchState& out, cudaStream_t st) {
   const size_t PK = (size_t)d->n_replicas * d->n_walkers;
   const size_t N = d->n_atoms_max, M = d->n_moves;
   struct F {
@@ -839,7 +998,6 @@ int clone_state(const JrDims* d, const JrParams* p, const JrStateBuffers* s,
       {s->iteration, (size_t)d->n_replicas * 4, (void**)&out.b.iteration},
       {s->emax, (size_t)d->n_replicas * 8, (void**)&out.b.emax},
   };
-  (void)p;
   for (auto& f : fields) {
     void* q = out.take(f.bytes);
     if (!q) return fail(JR_ERR_CUDA, "autotune scratch allocation failed");
@@ -860,49 +1018,50 @@ extern "C" int jr_autotune(const JrDims* dims, const JrParams* params,
   if (!state || !best || n_iter_probe < 1) return fail(JR_ERR_PARAM, "autotune arguments");
   cudaStream_t st = (cudaStream_t)stream;
   ScratchState scratch;
-  rc = clone_state(dims, params, state, scratch, st);
+  rc = clone_state(dims, state, scratch, st);
   if (rc) return rc;
-  void* ws = scratch.take(jr_ns_iterate_workspace_size(dims));
+  const size_t wsb = jr_ns_iterate_workspace_size(dims);
+  void* ws = scratch.take(wsb);
   if (!ws) return fail(JR_ERR_CUDA, "autotune workspace allocation failed");
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const int W = 1 + dims->n_extra;
   float best_ms = 1e30f;
   JrLaunchConfig bc = heuristic_config(dims);
-  const int thread_opts[] = {128, 256, 512};
-  const int tpa_opts[] = {2, 4, 8, 16, 32};
-  const int cluster_opts[] = {1, 2, 4, 8, 10, 12, 16};
-  for (int th : thread_opts) {
-    if (th / 32 > jr::kMaxWarps) continue;
-    for (int tpa : tpa_opts) {
-      if (tpa > th) continue;
-      // keep at least one pass worth of atoms busy
-      if (th / tpa > 4 * dims->n_atoms_max && tpa < 32) continue;
-      for (int cl : cluster_opts) {
-        if (cl > 1 && cl < 2 * W && cl != W) continue;
-        JrLaunchConfig c{th, tpa, cl};
-        if (check_config(c, dims) != JR_OK) continue;
-        // warm-up launch (also rejects shapes the hardware cannot place)
-        rc = jr_ns_iterate(dims, params, &scratch.b, nullptr, 1, &c, ws, 256, stream);
-        if (rc != JR_OK || cudaStreamSynchronize(st) != cudaSuccess) {
-          cudaGetLastError();
-          continue;
-        }
-        cudaEventRecord(e0, st);
-        rc = jr_ns_iterate(dims, params, &scratch.b, nullptr, n_iter_probe, &c, ws, 256, stream);
-        cudaEventRecord(e1, st);
-        if (rc != JR_OK || cudaEventSynchronize(e1) != cudaSuccess) {
-          cudaGetLastError();
-          continue;
-        }
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best_ms) {
-          best_ms = ms;
-          bc = c;
-        }
-      }
+  const int nmax = dims->n_atoms_max;
+  JrLaunchConfig cands[96];
+  int nc = 0;
+  const int clusters[] = {1, 2, 4, 8, 12, 16};
+  if (nmax <= 64) {  // warp walkers: 1..8 walkers per CTA
+    for (int wpc : {1, 2, 4})
+      for (int cl : clusters) cands[nc++] = JrLaunchConfig{32 * wpc, warp_tpa(nmax), cl, 1};
+  }
+  for (int th : {128, 256, 512})
+    for (int cl : clusters) {
+      int tpa = pow2_floor(th / nmax);
+      tpa = tpa > 16 ? 16 : (tpa < 1 ? 1 : tpa);
+      if (nc < 96) cands[nc++] = JrLaunchConfig{th, tpa, cl, 0};
+    }
+  for (int i = 0; i < nc; ++i) {
+    const JrLaunchConfig c = cands[i];
+    if (check_config(c, dims) != JR_OK) continue;
+    rc = jr_ns_iterate(dims, params, &scratch.b, nullptr, 1, &c, ws, wsb, stream);
+    if (rc != JR_OK || cudaStreamSynchronize(st) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    cudaEventRecord(e0, st);
+    rc = jr_ns_iterate(dims, params, &scratch.b, nullptr, n_iter_probe, &c, ws, wsb, stream);
+    cudaEventRecord(e1, st);
+    if (rc != JR_OK || cudaEventSynchronize(e1) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) {
+      best_ms = ms;
+      bc = c;
     }
   }
   cudaEventDestroy(e0);
@@ -914,37 +1073,5 @@ extern "C" int jr_autotune(const JrDims* dims, const JrParams* params,
   }
   *best = bc;
   g_last_error.clear();
-  return JR_OK;
-}
-
-// ======================================================= measurement ====
-namespace jr {
-// Independent FMA chains per thread: the FP32 FMA pipe's attainable rate.
-__global__ void __launch_bounds__(256) fma_peak_kernel(float* out, int iters) {
-  float a0 = threadIdx.x * 1e-7f, a1 = a0 + 1e-7f, a2 = a0 + 2e-7f, a3 = a0 + 3e-7f;
-  float a4 = a0 + 4e-7f, a5 = a0 + 5e-7f, a6 = a0 + 6e-7f, a7 = a0 + 7e-7f;
-  const float b = 0.999999f, c = 1e-7f;
-  for (int i = 0; i < iters; ++i) {
-#pragma unroll
-    for (int u = 0; u < 16; ++u) {
-      a0 = __fmaf_rn(a0, b, c); a1 = __fmaf_rn(a1, b, c);
-      a2 = __fmaf_rn(a2, b, c); a3 = __fmaf_rn(a3, b, c);
-      a4 = __fmaf_rn(a4, b, c); a5 = __fmaf_rn(a5, b, c);
-      a6 = __fmaf_rn(a6, b, c); a7 = __fmaf_rn(a7, b, c);
-    }
-  }
-  const float s = ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
-  if (s == 12345.678f) out[blockIdx.x] = s;  // keeps the chains live
-}
-}  // namespace jr
-
-extern "C" int jr_bench_fma_peak(int n_blocks, int iters, float* scratch, double* flops,
-                                 void* stream) {
-  if (n_blocks < 1 || iters < 1 || !scratch || !flops)
-    return fail(JR_ERR_PARAM, "fma_peak arguments");
-  jr::fma_peak_kernel<<<n_blocks, 256, 0, (cudaStream_t)stream>>>(scratch, iters);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_fail(e, "fma_peak launch");
-  *flops = 2.0 * 8.0 * 16.0 * (double)iters * 256.0 * (double)n_blocks;
   return JR_OK;
 }

@@ -1,13 +1,16 @@
-// jr_walk.cuh -- one walker resident in shared memory, walked by a whole CTA.
+// jr_walk.cuh -- one walker resident in shared memory, walked by a thread
+// group: a whole CTA (large walkers) or a single warp (small walkers, several
+// walkers per CTA).
 //
 // Arithmetic contract (shared with the CPU oracle's DEV mode):
 //   * pair terms in float32 with a fixed FMA placement (explicit intrinsics,
 //     the translation unit is compiled with -fmad=false),
 //   * every sum (energy, forces, norms, dot products) accumulated in float64
 //     and rounded to float32 once where a float32 value is needed.
-// Because the float64 sums of float32 terms are exact for any configuration
-// whose pair terms span < 2^29 in magnitude, results do not depend on the
-// thread mapping (launch shape) and match the oracle bit-for-bit.
+// The float64 sums of float32 terms are exact whenever a configuration's pair
+// terms span < 2^29 in magnitude, so results do not depend on the thread
+// mapping (launch shape) and match the oracle bit-for-bit; beyond that range
+// (overlapping atoms) float64 energies can differ in their last bit.
 #pragma once
 #include <cstdint>
 
@@ -17,6 +20,70 @@
 namespace jr {
 
 constexpr int kMaxWarps = 32;
+constexpr int kPairMatMax = 128;  // walkers up to this size use the pair buffer
+
+// ------------------------------------------------------------- groups ----
+
+// A whole CTA walking one walker.  sum3 reduces three doubles across the
+// block through two alternating shared buffers (one barrier per reduction).
+struct CtaGroup {
+  double (*red)[kMaxWarps][3];  // smem [2][kMaxWarps][3]
+  __device__ __forceinline__ int rank() const { return threadIdx.x; }
+  __device__ __forceinline__ int size() const { return blockDim.x; }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+  __device__ __forceinline__ bool leader() const { return threadIdx.x == 0; }
+  // lanes hold partials only at multiples of `stride` (a power of two)
+  __device__ __forceinline__ void sum3(double& a, double& b, double& c, int stride,
+                                       int& par) const {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int off = 16; off >= stride; off >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, off);
+      b += __shfl_xor_sync(0xffffffffu, b, off);
+      c += __shfl_xor_sync(0xffffffffu, c, off);
+    }
+    double (*buf)[3] = red[par];
+    if (lane == 0) {
+      buf[warp][0] = a;
+      buf[warp][1] = b;
+      buf[warp][2] = c;
+    }
+    __syncthreads();
+    a = 0.0;
+    b = 0.0;
+    c = 0.0;
+    for (int q = 0; q < nw; ++q) {
+      a += buf[q][0];
+      b += buf[q][1];
+      c += buf[q][2];
+    }
+    par ^= 1;
+  }
+};
+
+// One warp walking one walker: register shuffles only, no block barriers.
+struct WarpGroup {
+  __device__ __forceinline__ int rank() const { return threadIdx.x & 31; }
+  __device__ __forceinline__ int size() const { return 32; }
+  __device__ __forceinline__ void sync() const { __syncwarp(); }
+  __device__ __forceinline__ bool leader() const { return (threadIdx.x & 31) == 0; }
+  __device__ __forceinline__ void sum3(double& a, double& b, double& c, int stride,
+                                       int& par) const {
+    for (int off = 16; off >= stride; off >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, off);
+      b += __shfl_xor_sync(0xffffffffu, b, off);
+      c += __shfl_xor_sync(0xffffffffu, c, off);
+    }
+    if (stride > 1) {
+      a = __shfl_sync(0xffffffffu, a, 0);
+      b = __shfl_sync(0xffffffffu, b, 0);
+      c = __shfl_sync(0xffffffffu, c, 0);
+    }
+    (void)par;
+  }
+};
+
+// ----------------------------------------------------------- walker ----
 
 // Geometry of one cell: the matrix, its inverse and the image translations.
 struct CellCtx {
@@ -24,19 +91,16 @@ struct CellCtx {
   float h[9];    // the cell used for geometry (1e10*I when det == 0)
   float inv[9];
   int diag;
-  float vol;  // |det(h)| of the un-substituted cell (ensemble term)
+  float vol;  // |det| of the stored cell (ensemble term)
 };
 
-// Fixed-size per-CTA state; the per-atom arrays live in dynamic smem.
+// Per-walker scalar state (one per walking group).
 struct WalkShared {
-  CellCtx cc[2];        // [cur], [trial]
-  int cur;              // index of the current cell context
-  double E;             // current full potential of the walker
+  CellCtx cc[2];  // [cur], [trial]
+  int cur;        // index of the current cell context
+  double E;       // current full potential of the walker
   float step_sizes[JR_MAX_MOVES];
   int counts[JR_MAX_SPECIES];
-  float sig2[JR_MAX_SPECIES * JR_MAX_SPECIES];
-  float eps4[JR_MAX_SPECIES * JR_MAX_SPECIES];
-  float eps24[JR_MAX_SPECIES * JR_MAX_SPECIES];
   // per-walker MWG counters (MCState.n_accepted / n_proposed)
   int w_acc[JR_MAX_MOVES];
   int w_prop[JR_MAX_MOVES];
@@ -46,46 +110,103 @@ struct WalkShared {
   int c_rr[JR_MAX_MOVES * 4];
   int c_nev[JR_MAX_MOVES];
   int c_ngr[JR_MAX_MOVES];
-  double red[2][kMaxWarps][3];
-  int bcast_i[4];
-  float bcast_f[4];
 };
 
-// Dynamic shared memory carve-up for Nmax atoms and n_img images.
+// Pair tables of the model, shared by every walker of a CTA.
+struct PairTables {
+  float sig2[JR_MAX_SPECIES * JR_MAX_SPECIES];
+  float eps4[JR_MAX_SPECIES * JR_MAX_SPECIES];
+  float eps24[JR_MAX_SPECIES * JR_MAX_SPECIES];
+};
+
+// Per-walker arrays in dynamic shared memory.  Walkers with one image and at
+// most kPairMatMax atoms also get a compact upper-triangle buffer holding one
+// float4 (force term) per unordered pair; the pair decode table is shared by
+// all walkers of a CTA (same atom count).
 struct WalkArrays {
-  float4* xs;   // [Nmax] position + type bits (current / trial positions)
-  float* x0;    // [3 Nmax] saved positions
-  float* dir;   // [3 Nmax] direction
-  float* dp;    // [3 Nmax] perturbed direction (flip target on reject)
-  float* F;     // [3 Nmax] forces
-  float* T;     // [2][3 n_img] image translations for cc[0], cc[1]
+  float4* xs;           // [Nmax] position + type bits (current / trial positions)
+  float* x0;            // [3 Nmax] saved positions
+  float* dir;           // [3 Nmax] direction
+  float* dp;            // [3 Nmax] perturbed direction (flip target on reject)
+  float* F;             // [3 Nmax] forces
+  float* T;             // [2][3 n_img] image translations for cc[0], cc[1]
+  float4* pm;           // [Nmax(Nmax-1)/2] pair force terms, or nullptr
+  const uint16_t* pij;  // [Nmax(Nmax-1)/2] pair decode a | b << 8, or nullptr
 };
 
-__host__ __device__ inline size_t walk_dyn_smem_bytes(int nmax, int nimg) {
-  size_t b = 16u * (size_t)nmax + 4u * 12u * (size_t)nmax + 2u * 3u * 4u * (size_t)nimg;
-  return (b + 15) & ~(size_t)15;
+__host__ __device__ inline bool use_pair_matrix(int nmax, int nimg) {
+  return nimg == 1 && nmax <= kPairMatMax;
 }
 
-__device__ inline WalkArrays carve(void* dyn, int nmax, int nimg) {
-  WalkArrays a;
-  char* p = (char*)dyn;
+__host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+__host__ __device__ inline size_t pair_count(int nmax) {
+  return (size_t)nmax * (size_t)(nmax - 1) / 2;
+}
+
+// Bytes of one walker: WalkShared + arrays (+ pair buffer).
+__host__ __device__ inline size_t walker_smem_bytes(int nmax, int nimg) {
+  size_t b = align16(sizeof(WalkShared));
+  b += 16u * (size_t)nmax + 4u * 12u * (size_t)nmax;
+  b += align16(2u * 3u * 4u * (size_t)nimg);
+  if (use_pair_matrix(nmax, nimg)) b += 16u * pair_count(nmax);
+  return align16(b);
+}
+
+// Bytes of the CTA-shared pair decode table.
+__host__ __device__ inline size_t pair_table_bytes(int nmax, int nimg) {
+  return use_pair_matrix(nmax, nimg) ? align16(2u * pair_count(nmax)) : 0;
+}
+
+__device__ inline WalkShared* carve_walker(char* p, int nmax, int nimg, const uint16_t* pij,
+                                           WalkArrays& a) {
+  WalkShared* s = reinterpret_cast<WalkShared*>(p);
+  p += align16(sizeof(WalkShared));
   a.xs = (float4*)p; p += 16 * nmax;
   a.x0 = (float*)p; p += 12 * nmax;
   a.dir = (float*)p; p += 12 * nmax;
   a.dp = (float*)p; p += 12 * nmax;
   a.F = (float*)p; p += 12 * nmax;
-  a.T = (float*)p;
-  return a;
+  a.T = (float*)p; p += align16(2 * 3 * 4 * nimg);
+  if (use_pair_matrix(nmax, nimg)) {
+    a.pm = (float4*)p;
+    a.pij = pij;
+  } else {
+    a.pm = nullptr;
+    a.pij = nullptr;
+  }
+  return s;
 }
 
-// Per-thread view of the walker: the shared state, the smem arrays, the atom
-// count, the pair-loop mapping and this thread's copy of the reduction-buffer
-// parity (block-uniform, flipped by every block reduction).
+// Fill the pair decode table for n atoms (pairs a < b, row-major), CTA-wide.
+__device__ inline void build_pair_table(uint16_t* pij, int n) {
+  if (!pij) return;
+  const int np = n * (n - 1) / 2;
+  for (int p = threadIdx.x; p < np; p += blockDim.x) {
+    int a = (int)((2.0f * n - 1.0f - sqrtf((2.0f * n - 1.0f) * (2.0f * n - 1.0f) - 8.0f * p)) * 0.5f);
+    if (a < 0) a = 0;
+    if (a > n - 2) a = n - 2;
+    while (a > 0 && a * (2 * n - a - 1) / 2 > p) --a;
+    while (a < n - 2 && (a + 1) * (2 * n - a - 2) / 2 <= p) ++a;
+    const int b = p - a * (2 * n - a - 1) / 2 + a + 1;
+    pij[p] = (uint16_t)(a | (b << 8));
+  }
+}
+
+__device__ __forceinline__ int pair_index(int a, int b, int n) {
+  return a * (2 * n - a - 1) / 2 + (b - a - 1);
+}
+
+// Per-thread view of one walker and the group that walks it.  `par` is this
+// thread's copy of the block-reduction buffer parity (group-uniform).
+template <class G>
 struct Walker {
   WalkShared& s;
   WalkArrays arr;
+  const PairTables& tab;
   int n;
   int tpa;
+  G g;
   int par;
 };
 
@@ -111,8 +232,8 @@ __device__ __forceinline__ float det3(const float* a) {
 
 // Fill a cell context: det==0 substitutes 1e10*I (lj.py:136-137); a diagonal
 // cell inverts with float32 division, any other through the double adjugate.
-__device__ inline void make_cell_ctx(const float* h_in, CellCtx& cc,
-                                     float* T, const JrModelParams& mp) {
+__device__ inline void make_cell_ctx(const float* h_in, CellCtx& cc, float* T,
+                                     const JrModelParams& mp) {
   cc.vol = fabsf(det3(h_in));
   for (int q = 0; q < 9; ++q) cc.raw[q] = h_in[q];
   float h[9];
@@ -160,9 +281,10 @@ __device__ inline void make_cell_ctx(const float* h_in, CellCtx& cc,
   }
 }
 
-// Triclinic minimum image: dr - round(dr @ inv) @ h (lj.py:147-154).
-__device__ __forceinline__ void mic(const CellCtx& cc, float& dx, float& dy,
-                                    float& dz) {
+// Triclinic minimum image: dr - round(dr @ inv) @ h (lj.py:147-154).  The
+// diagonal branch is the general formula with the zero terms dropped, which
+// leaves every result bit unchanged.
+__device__ __forceinline__ void mic(const CellCtx& cc, float& dx, float& dy, float& dz) {
   if (cc.diag) {
     float n0 = rintf(__fmul_rn(dx, cc.inv[0]));
     float n1 = rintf(__fmul_rn(dy, cc.inv[4]));
@@ -193,63 +315,104 @@ __device__ __forceinline__ void mic(const CellCtx& cc, float& dx, float& dy,
   }
 }
 
+// Register copy of the geometry the minimum image needs; for a diagonal cell
+// only the six diagonal entries are read (the rest are never loaded).
+struct MicRegs {
+  float inv[9];
+  float h[9];
+};
+
+template <bool kDiag>
+__device__ __forceinline__ MicRegs load_mic(const CellCtx& cc) {
+  MicRegs m;
+  if (kDiag) {
+    m.inv[0] = cc.inv[0]; m.inv[4] = cc.inv[4]; m.inv[8] = cc.inv[8];
+    m.h[0] = cc.h[0]; m.h[4] = cc.h[4]; m.h[8] = cc.h[8];
+  } else {
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      m.inv[q] = cc.inv[q];
+      m.h[q] = cc.h[q];
+    }
+  }
+  return m;
+}
+
+// mic() with the cell in registers; bit-identical to mic() for either branch.
+template <bool kDiag>
+__device__ __forceinline__ void mic_r(const MicRegs& m, float& dx, float& dy, float& dz) {
+  if (kDiag) {
+    const float n0 = rintf(__fmul_rn(dx, m.inv[0]));
+    const float n1 = rintf(__fmul_rn(dy, m.inv[4]));
+    const float n2 = rintf(__fmul_rn(dz, m.inv[8]));
+    dx = __fsub_rn(dx, __fmul_rn(n0, m.h[0]));
+    dy = __fsub_rn(dy, __fmul_rn(n1, m.h[4]));
+    dz = __fsub_rn(dz, __fmul_rn(n2, m.h[8]));
+  } else {
+    float n[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      float f = __fmul_rn(dx, m.inv[q]);
+      f = __fmaf_rn(dy, m.inv[3 + q], f);
+      f = __fmaf_rn(dz, m.inv[6 + q], f);
+      n[q] = rintf(f);
+    }
+    float sh[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      float v = __fmul_rn(n[0], m.h[q]);
+      v = __fmaf_rn(n[1], m.h[3 + q], v);
+      v = __fmaf_rn(n[2], m.h[6 + q], v);
+      sh[q] = v;
+    }
+    dx = __fsub_rn(dx, sh[0]);
+    dy = __fsub_rn(dy, sh[1]);
+    dz = __fsub_rn(dz, sh[2]);
+  }
+}
+
+// 1/x for the pair loop: a bit-pattern seed refined by three Newton-Raphson
+// steps y <- y + y*(1 - x*y), all in fused multiply-adds, so the result is the
+// same on any IEEE machine with an FMA (the CPU check reproduces it bit for
+// bit).  Max error 0.501 ulp over normal inputs; inputs outside [2^-120, 2^120]
+// (zero, denormals, inf, NaN) take the correctly rounded reciprocal.
+__device__ __forceinline__ float rcp_nr(float x) {
+  float y = __int_as_float(0x7EF311C3 - __float_as_int(x));
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float e = __fmaf_rn(-x, y, 1.0f);
+    y = __fmaf_rn(y, e, y);
+  }
+  if (!(x >= 0x1p-120f && x <= 0x1p120f)) y = __frcp_rn(x);  // rare
+  return y;
+}
+
 // One LJ pair term (lj.py:191-203), float32: energy e and the force
-// coefficient g with F_i += g * dr_ij.
-__device__ __forceinline__ void lj_pair(float dx, float dy, float dz,
-                                        float sig2, float eps4, float eps24,
-                                        bool has_cut, float rc2, float& e,
+// coefficient g with F_i += g * dr_ij; e = g = 0 beyond the cutoff.  Written
+// branch-free (compute, then select) so a warp never splits on the cutoff.
+__device__ __forceinline__ void lj_pair(float dx, float dy, float dz, float sig2, float eps4,
+                                        float eps24, bool has_cut, float rc2, float& e,
                                         float& g) {
   float r2 = __fmul_rn(dx, dx);
   r2 = __fmaf_rn(dy, dy, r2);
   r2 = __fmaf_rn(dz, dz, r2);
-  if (has_cut && !(r2 < rc2)) {
-    e = 0.0f;
-    g = 0.0f;
-    return;
-  }
-  float ri = __frcp_rn(r2);
-  float s2 = __fmul_rn(sig2, ri);
-  float s4 = __fmul_rn(s2, s2);
-  float s6 = __fmul_rn(s4, s2);
-  float s12 = __fmul_rn(s6, s6);
-  e = __fmul_rn(eps4, __fsub_rn(s12, s6));
-  float t = __fmaf_rn(2.0f, s12, -s6);
-  float a = __fmul_rn(eps24, ri);
-  g = -__fmul_rn(a, t);
-}
-
-// Block-wide sum of three doubles; lanes hold partials only at multiples of
-// `lane_stride` (a power of two).  Deterministic: warps summed in order.  The
-// two partial buffers alternate, so one barrier per reduction suffices.
-__device__ __forceinline__ void block_sum3(Walker& w, double& a, double& b,
-                                           double& c, int lane_stride) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nw = (blockDim.x + 31) >> 5;
-  for (int off = 16; off >= lane_stride; off >>= 1) {
-    a += __shfl_xor_sync(0xffffffffu, a, off);
-    b += __shfl_xor_sync(0xffffffffu, b, off);
-    c += __shfl_xor_sync(0xffffffffu, c, off);
-  }
-  double (*buf)[3] = w.s.red[w.par];
-  if (lane == 0) {
-    buf[warp][0] = a;
-    buf[warp][1] = b;
-    buf[warp][2] = c;
-  }
-  __syncthreads();
-  a = 0.0; b = 0.0; c = 0.0;
-  for (int q = 0; q < nw; ++q) {
-    a += buf[q][0];
-    b += buf[q][1];
-    c += buf[q][2];
-  }
-  w.par ^= 1;
+  const bool inside = !has_cut || (r2 < rc2);
+  const float ri = rcp_nr(r2);
+  const float s2 = __fmul_rn(sig2, ri);
+  const float s4 = __fmul_rn(s2, s2);
+  const float s6 = __fmul_rn(s4, s2);
+  const float s12 = __fmul_rn(s6, s6);
+  const float ev = __fmul_rn(eps4, __fsub_rn(s12, s6));
+  const float t = __fmaf_rn(2.0f, s12, -s6);
+  const float a = __fmul_rn(eps24, ri);
+  const float gv = -__fmul_rn(a, t);
+  e = inside ? ev : 0.0f;
+  g = inside ? gv : 0.0f;
 }
 
 // Ensemble term P*V - mu*N (ensemble.py:34-59) in float64.
-__device__ __forceinline__ double ensemble_term(const WalkShared& s, float vol,
-                                                float pressure, const float* mu,
-                                                int nsp) {
+__device__ __forceinline__ double ensemble_term(const WalkShared& s, float vol, float pressure,
+                                                const float* mu, int nsp) {
   double e = (double)pressure * (double)vol;
   if (mu) {
     double dot = 0.0;
@@ -260,8 +423,8 @@ __device__ __forceinline__ double ensemble_term(const WalkShared& s, float vol,
 }
 
 // Gaussian-mixture toy (toy.py:163-204), float64, forces rounded to float32.
-__device__ inline double gauss_mix_energy(const JrModelParams& mp, const float4* xs,
-                                          int n, float* F, bool forces) {
+__device__ inline double gauss_mix_energy(const JrModelParams& mp, const float4* xs, int n,
+                                          float* F, bool forces) {
   double com[3] = {0, 0, 0};
   for (int i = 0; i < n; ++i) {
     com[0] += (double)xs[i].x;
@@ -304,68 +467,164 @@ __device__ __forceinline__ int center_image(const JrModelParams& mp) {
   return -1;
 }
 
-// Model energy U (forces into arr.F when kForces) of the walker in smem; also
-// returns sum(F^2) and sum(F . dir) for the galilean reflection.  All threads
-// call it; the results are block-uniform on return.
-template <bool kForces>
-__device__ void model_eval(const JrParams& P, Walker& w, int cidx, double& U,
-                           double& sff, double& sfd) {
-  WalkShared& s = w.s;
+// Force gather contract: F_i is accumulated in float32 in a canonical order
+// that depends only on n -- partners j in blocks of 8 (sequential, ascending
+// j, then ascending image), then the block partials combined pairwise
+// ((P0+P1)+(P2+P3))+... over L = next_pow2(ceil(n/8)) lanes.  The lanes of
+// one atom are adjacent in a warp; the pairwise tree is the xor butterfly.
+__device__ __forceinline__ int gather_lanes(int n) {
+  const int nb = (n + 7) >> 3;
+  int L = 1;
+  while (L < nb) L <<= 1;
+  return L;
+}
+
+__device__ __forceinline__ void gather_tree(float& fx, float& fy, float& fz, int L) {
+  for (int off = 1; off < L; off <<= 1) {
+    fx = __fadd_rn(fx, __shfl_xor_sync(0xffffffffu, fx, off));
+    fy = __fadd_rn(fy, __shfl_xor_sync(0xffffffffu, fy, off));
+    fz = __fadd_rn(fz, __shfl_xor_sync(0xffffffffu, fz, off));
+  }
+}
+
+// Unordered pairs a < b once each (pair buffer path): the force term g*dr of
+// pair p goes to arr.pm[p]; atom i then gathers +pm[p(i,j)] for j > i and
+// -pm[p(j,i)] for j < i in float64 (the float32 term of the mirrored ordered
+// pair is exactly the negation).  U is the float64 sum over pairs.
+template <bool kForces, bool kS1, bool kDiag, class G>
+__device__ __forceinline__ void pairs_matrix(const JrParams& P, Walker<G>& w, const MicRegs& cc,
+                                             double& U, double& sff, double& sfd) {
   const WalkArrays& arr = w.arr;
-  const int n = w.n, tpa = w.tpa;
-  const JrModelParams& mp = P.model;
-  if (mp.model == JR_MODEL_GAUSS_MIX) {
-    double e = 0.0, a = 0.0, b = 0.0;
-    if (threadIdx.x == 0) {
-      e = gauss_mix_energy(mp, arr.xs, n, arr.F, kForces);
-      if (kForces) {
-        for (int q = 0; q < 3 * n; ++q) {
-          a += (double)arr.F[q] * (double)arr.F[q];
-          b += (double)arr.F[q] * (double)arr.dir[q];
-        }
-      }
+  const int n = w.n;
+  const int nsp = P.model.n_species;
+  const bool has_cut = P.model.has_cutoff != 0;
+  const float rc2 = P.model.rc2;
+  const float sig2_1 = w.tab.sig2[0], eps4_1 = w.tab.eps4[0], eps24_1 = w.tab.eps24[0];
+  const int np = n * (n - 1) / 2;
+  const int tid = w.g.rank(), gs = w.g.size();
+  double ep = 0.0;
+#pragma unroll 2
+  for (int p = tid; p < np; p += gs) {
+    const uint32_t ab = arr.pij[p];
+    const int a = ab & 255, b = ab >> 8;
+    const float4 xa = arr.xs[a], xb = arr.xs[b];
+    float dx = __fsub_rn(xb.x, xa.x);
+    float dy = __fsub_rn(xb.y, xa.y);
+    float dz = __fsub_rn(xb.z, xa.z);
+    mic_r<kDiag>(cc, dx, dy, dz);
+    float sig2 = sig2_1, eps4 = eps4_1, eps24 = eps24_1;
+    if (!kS1) {
+      const int pt = __float_as_int(xa.w) * nsp + __float_as_int(xb.w);
+      sig2 = w.tab.sig2[pt];
+      eps4 = w.tab.eps4[pt];
+      eps24 = w.tab.eps24[pt];
     }
-    block_sum3(w, e, a, b, 1);
-    U = e;
-    sff = a;
-    sfd = b;
+    float e, g;
+    lj_pair(dx, dy, dz, sig2, eps4, eps24, has_cut, rc2, e, g);
+    ep += (double)e;
+    if (kForces)
+      arr.pm[p] = make_float4(__fmul_rn(g, dx), __fmul_rn(g, dy), __fmul_rn(g, dz), 0.0f);
+  }
+  if (!kForces) {
+    double z0 = 0.0, z1 = 0.0;
+    w.g.sum3(ep, z0, z1, 1, w.par);
+    U = ep;
+    sff = 0.0;
+    sfd = 0.0;
     return;
   }
-  const CellCtx& cc = s.cc[cidx];
-  const float* T = arr.T + cidx * 3 * mp.n_images;
+  w.g.sync();
+  const int L = gather_lanes(n);
+  const int apb = gs / L;
+  const int blk = tid & (L - 1);
+  double ff_part = 0.0, fd_part = 0.0;
+  for (int base = 0; base < n; base += apb) {
+    const int i = base + tid / L;
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+    // partners j0..j0+7 in ascending order; an absent partner adds +0, which
+    // leaves the running sum unchanged (it is never -0)
+    const int j0 = blk * 8;
+#pragma unroll
+    for (int jj = 0; jj < 8; ++jj) {
+      const int j = j0 + jj;
+      const bool ok = (i < n) && (j < n) && (j != i);
+      const bool up = i < j;
+      const int idx = ok ? (up ? pair_index(i, j, n) : pair_index(j, i, n)) : 0;
+      const float4 v = ok ? arr.pm[idx] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      const float vx = ok ? (up ? v.x : -v.x) : 0.0f;
+      const float vy = ok ? (up ? v.y : -v.y) : 0.0f;
+      const float vz = ok ? (up ? v.z : -v.z) : 0.0f;
+      fx = __fadd_rn(fx, vx);
+      fy = __fadd_rn(fy, vy);
+      fz = __fadd_rn(fz, vz);
+    }
+    gather_tree(fx, fy, fz, L);
+    if (blk == 0 && i < n) {
+      arr.F[3 * i] = fx;
+      arr.F[3 * i + 1] = fy;
+      arr.F[3 * i + 2] = fz;
+      ff_part += (double)fx * (double)fx + (double)fy * (double)fy + (double)fz * (double)fz;
+      fd_part += (double)fx * (double)arr.dir[3 * i] + (double)fy * (double)arr.dir[3 * i + 1] +
+                 (double)fz * (double)arr.dir[3 * i + 2];
+    }
+  }
+  double e_part = ep;
+  w.g.sum3(e_part, ff_part, fd_part, 1, w.par);
+  U = e_part;
+  sff = ff_part;
+  sfd = fd_part;
+}
+
+// Ordered pairs (i, j), every image; gather_lanes(n) lanes per atom i, each
+// lane one block of 8 partners (the canonical gather order above).
+template <bool kForces, bool kS1, bool kDiag, class G>
+__device__ __forceinline__ void pairs_ordered(const JrParams& P, Walker<G>& w, const MicRegs& cc,
+                                              const float* T, double& U, double& sff,
+                                              double& sfd) {
+  const WalkArrays& arr = w.arr;
+  const int n = w.n;
+  const JrModelParams& mp = P.model;
   const int nimg = mp.n_images;
   const bool has_cut = mp.has_cutoff != 0;
   const float rc2 = mp.rc2;
   const int nsp = mp.n_species;
-  const int tid = threadIdx.x;
-  const int apb = blockDim.x / tpa;
-  const int g0 = tid % tpa;
+  const float sig2_1 = w.tab.sig2[0], eps4_1 = w.tab.eps4[0], eps24_1 = w.tab.eps24[0];
+  const int tid = w.g.rank();
+  const int L = gather_lanes(n);
+  const int apb = w.g.size() / L;
+  const int blk = tid & (L - 1);
   const int center = center_image(mp);
   double e_part = 0.0, ff_part = 0.0, fd_part = 0.0;
   for (int base = 0; base < n; base += apb) {
-    const int i = base + tid / tpa;
-    double fx = 0.0, fy = 0.0, fz = 0.0, ei = 0.0;
+    const int i = base + tid / L;
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
     if (i < n) {
       const float4 xi = arr.xs[i];
       const int ti = __float_as_int(xi.w);
-      for (int j = g0; j < n; j += tpa) {
+      const int j0 = blk * 8;
+      const int j1 = j0 + 8 < n ? j0 + 8 : n;
+      for (int j = j0; j < j1; ++j) {
         const float4 xj = arr.xs[j];
-        const int tj = __float_as_int(xj.w);
         float dx = __fsub_rn(xj.x, xi.x);
         float dy = __fsub_rn(xj.y, xi.y);
         float dz = __fsub_rn(xj.z, xi.z);
-        mic(cc, dx, dy, dz);
-        const int pt = ti * nsp + tj;
-        const float sig2 = s.sig2[pt], eps4 = s.eps4[pt], eps24 = s.eps24[pt];
+        mic_r<kDiag>(cc, dx, dy, dz);
+        float sig2 = sig2_1, eps4 = eps4_1, eps24 = eps24_1;
+        if (!kS1) {
+          const int pt = ti * nsp + __float_as_int(xj.w);
+          sig2 = w.tab.sig2[pt];
+          eps4 = w.tab.eps4[pt];
+          eps24 = w.tab.eps24[pt];
+        }
         if (nimg == 1) {
           if (j != i) {
             float e, g;
             lj_pair(dx, dy, dz, sig2, eps4, eps24, has_cut, rc2, e, g);
-            ei += (double)e;
+            e_part += (double)e;
             if (kForces) {
-              fx += (double)__fmul_rn(g, dx);
-              fy += (double)__fmul_rn(g, dy);
-              fz += (double)__fmul_rn(g, dz);
+              fx = __fadd_rn(fx, __fmul_rn(g, dx));
+              fy = __fadd_rn(fy, __fmul_rn(g, dy));
+              fz = __fadd_rn(fz, __fmul_rn(g, dz));
             }
           }
         } else {
@@ -376,60 +635,101 @@ __device__ void model_eval(const JrParams& P, Walker& w, int cidx, double& U,
             const float ez = __fadd_rn(dz, T[3 * k + 2]);
             float e, g;
             lj_pair(ex, ey, ez, sig2, eps4, eps24, has_cut, rc2, e, g);
-            ei += (double)e;
+            e_part += (double)e;
             if (kForces && i != j) {
-              fx += (double)__fmul_rn(g, ex);
-              fy += (double)__fmul_rn(g, ey);
-              fz += (double)__fmul_rn(g, ez);
+              fx = __fadd_rn(fx, __fmul_rn(g, ex));
+              fy = __fadd_rn(fy, __fmul_rn(g, ey));
+              fz = __fadd_rn(fz, __fmul_rn(g, ez));
             }
           }
         }
       }
     }
-    for (int off = tpa >> 1; off > 0; off >>= 1) {
-      ei += __shfl_xor_sync(0xffffffffu, ei, off);
-      if (kForces) {
-        fx += __shfl_xor_sync(0xffffffffu, fx, off);
-        fy += __shfl_xor_sync(0xffffffffu, fy, off);
-        fz += __shfl_xor_sync(0xffffffffu, fz, off);
-      }
-    }
-    if (g0 == 0 && i < n) {
-      e_part += ei;
-      if (kForces) {
-        const float Fx = __double2float_rn(fx), Fy = __double2float_rn(fy),
-                    Fz = __double2float_rn(fz);
-        arr.F[3 * i] = Fx;
-        arr.F[3 * i + 1] = Fy;
-        arr.F[3 * i + 2] = Fz;
-        ff_part += (double)Fx * (double)Fx + (double)Fy * (double)Fy +
-                   (double)Fz * (double)Fz;
-        fd_part += (double)Fx * (double)arr.dir[3 * i] +
-                   (double)Fy * (double)arr.dir[3 * i + 1] +
-                   (double)Fz * (double)arr.dir[3 * i + 2];
+    if (kForces) {
+      gather_tree(fx, fy, fz, L);
+      if (blk == 0 && i < n) {
+        arr.F[3 * i] = fx;
+        arr.F[3 * i + 1] = fy;
+        arr.F[3 * i + 2] = fz;
+        ff_part += (double)fx * (double)fx + (double)fy * (double)fy + (double)fz * (double)fz;
+        fd_part += (double)fx * (double)arr.dir[3 * i] + (double)fy * (double)arr.dir[3 * i + 1] +
+                   (double)fz * (double)arr.dir[3 * i + 2];
       }
     }
   }
-  block_sum3(w, e_part, ff_part, fd_part, tpa);
+  w.g.sum3(e_part, ff_part, fd_part, 1, w.par);
   U = 0.5 * e_part;
   sff = ff_part;
   sfd = fd_part;
 }
 
+// Model energy U (forces into arr.F when kForces) of the walker; also sum(F^2)
+// and sum(F . dir) for the galilean reflection.  Results are group-uniform.
+template <bool kForces, class G>
+__device__ __forceinline__ void model_eval(const JrParams& P, Walker<G>& w, int cidx, double& U, double& sff,
+                           double& sfd) {
+  const WalkArrays& arr = w.arr;
+  const JrModelParams& mp = P.model;
+  if (mp.model == JR_MODEL_GAUSS_MIX) {
+    double e = 0.0, a = 0.0, b = 0.0;
+    if (w.g.leader()) {
+      e = gauss_mix_energy(mp, arr.xs, w.n, arr.F, kForces);
+      if (kForces) {
+        for (int q = 0; q < 3 * w.n; ++q) {
+          a += (double)arr.F[q] * (double)arr.F[q];
+          b += (double)arr.F[q] * (double)arr.dir[q];
+        }
+      }
+    }
+    w.g.sum3(e, a, b, 1, w.par);
+    U = e;
+    sff = a;
+    sfd = b;
+    w.g.sync();
+    return;
+  }
+  const CellCtx& ccs = w.s.cc[cidx];
+  const bool s1 = mp.n_species == 1;
+  const bool diag = ccs.diag != 0;
+  if (arr.pm != nullptr && mp.n_images == 1 && w.n <= kPairMatMax) {
+    if (diag) {
+      const MicRegs cc = load_mic<true>(ccs);
+      if (s1) pairs_matrix<kForces, true, true>(P, w, cc, U, sff, sfd);
+      else pairs_matrix<kForces, false, true>(P, w, cc, U, sff, sfd);
+    } else {
+      const MicRegs cc = load_mic<false>(ccs);
+      if (s1) pairs_matrix<kForces, true, false>(P, w, cc, U, sff, sfd);
+      else pairs_matrix<kForces, false, false>(P, w, cc, U, sff, sfd);
+    }
+  } else {
+    const float* T = arr.T + cidx * 3 * mp.n_images;
+    if (diag) {
+      const MicRegs cc = load_mic<true>(ccs);
+      if (s1) pairs_ordered<kForces, true, true>(P, w, cc, T, U, sff, sfd);
+      else pairs_ordered<kForces, false, true>(P, w, cc, T, U, sff, sfd);
+    } else {
+      const MicRegs cc = load_mic<false>(ccs);
+      if (s1) pairs_ordered<kForces, true, false>(P, w, cc, T, U, sff, sfd);
+      else pairs_ordered<kForces, false, false>(P, w, cc, T, U, sff, sfd);
+    }
+  }
+}
+
 // Full potential of the walker for cell context cidx: U + (P*V - mu*N).
-template <bool kForces>
-__device__ __forceinline__ double ham_eval(const JrParams& P, Walker& w, int cidx,
-                                           float pressure, const float* mu,
-                                           double& sff, double& sfd) {
+template <bool kForces, class G>
+__device__ __forceinline__ double ham_eval(const JrParams& P, Walker<G>& w, int cidx,
+                                           float pressure, const float* mu, double& sff,
+                                           double& sfd) {
   double U;
   model_eval<kForces>(P, w, cidx, U, sff, sfd);
   if (P.model.model == JR_MODEL_GAUSS_MIX) return U;
   return U + ensemble_term(w.s, w.s.cc[cidx].vol, pressure, mu, P.model.n_species);
 }
 
-__device__ __forceinline__ double block_sum1(Walker& w, double v) {
+template <class G>
+__device__ __forceinline__ double group_sum1(Walker<G>& w, double v) {
   double b = 0.0, c = 0.0;
-  block_sum3(w, v, b, c, 1);
+  w.g.sum3(v, b, c, 1, w.par);
   return v;
 }
 
@@ -438,19 +738,19 @@ __device__ __forceinline__ double block_sum1(Walker& w, double v) {
 // Galilean move (galilean.py:142-300) with forces-based reflection.  The
 // reflection d - 2 (f.d) f with f = F/|F| is evaluated as
 // d - [2 (F.d) / max(|F|,1e-10)^2] F from two float64 sums.
-__device__ bool move_galilean(const JrParams& P, Walker& w, Key key, float step,
-                              int R, float pa, double emax, float pressure,
-                              const float* mu) {
+template <class G>
+__device__ __forceinline__ bool move_galilean(const JrParams& P, Walker<G>& w, Key key, float step, int R,
+                              float pa, double emax, float pressure, const float* mu) {
   const WalkArrays& arr = w.arr;
   const int n3 = 3 * w.n;
+  const int r0 = w.g.rank(), gs = w.g.size();
   const Key ki = split(key, 0u), kp = split(key, 1u);
   double sq = 0.0;
-  for (int q = threadIdx.x; q < n3; q += blockDim.x)
-    sq += (double)arr.dir[q] * (double)arr.dir[q];
-  sq = block_sum1(w, sq);
+  for (int q = r0; q < n3; q += gs) sq += (double)arr.dir[q] * (double)arr.dir[q];
+  sq = group_sum1(w, sq);
   const bool fresh = __double2float_rn(sqrt(sq)) < 1e-8f;
   double sv = 0.0;
-  for (int q = threadIdx.x; q < n3; q += blockDim.x) {
+  for (int q = r0; q < n3; q += gs) {
     float v;
     if (fresh) {
       v = normal(bits32(ki, (uint32_t)q));
@@ -460,10 +760,10 @@ __device__ bool move_galilean(const JrParams& P, Walker& w, Key key, float step,
     arr.dir[q] = v;
     sv += (double)v * (double)v;
   }
-  sv = block_sum1(w, sv);
+  sv = group_sum1(w, sv);
   const float nv = __double2float_rn(sqrt(sv));
   const float den = nv > 1e-10f ? nv : 1e-10f;
-  for (int q = threadIdx.x; q < n3; q += blockDim.x) {
+  for (int q = r0; q < n3; q += gs) {
     const float v = __fdiv_rn(arr.dir[q], den);
     arr.dir[q] = v;
     arr.dp[q] = v;
@@ -472,32 +772,31 @@ __device__ bool move_galilean(const JrParams& P, Walker& w, Key key, float step,
   const double E0 = w.s.E;
   double E = E0;
   for (int r = 0; r < R; ++r) {
-    for (int q = threadIdx.x; q < n3; q += blockDim.x) {
+    for (int q = r0; q < n3; q += gs) {
       float& x = pos_at(arr.xs, q);
       x = __fmaf_rn(step, arr.dir[q], x);
     }
-    __syncthreads();
+    w.g.sync();
     double sff, sfd;
     E = ham_eval<true>(P, w, w.s.cur, pressure, mu, sff, sfd);
     if (isnan(E)) E = INFINITY;
     if (E >= emax) {
-      double nrm = sqrt(sff);
-      if (nrm < 1e-10) nrm = 1e-10;
-      const float coef = __double2float_rn(__ddiv_rn(2.0 * sfd, nrm * nrm));
-      for (int q = threadIdx.x; q < n3; q += blockDim.x)
-        arr.dir[q] = __fmaf_rn(-coef, arr.F[q], arr.dir[q]);
+      // d <- d - [2 (F.d) / max(|F|^2, 1e-20)] F, the scalar in float32
+      const float ffs = __double2float_rn(sff);
+      const float coef = __fmul_rn(2.0f * __double2float_rn(sfd), rcp_nr(ffs > 1e-20f ? ffs : 1e-20f));
+      for (int q = r0; q < n3; q += gs) arr.dir[q] = __fmaf_rn(-coef, arr.F[q], arr.dir[q]);
     }
   }
   const bool acc = E < emax;
   if (!acc) {
-    for (int q = threadIdx.x; q < n3; q += blockDim.x) {
+    for (int q = r0; q < n3; q += gs) {
       pos_at(arr.xs, q) = arr.x0[q];
       arr.dir[q] = -arr.dp[q];
     }
   }
-  __syncthreads();
-  if (threadIdx.x == 0) w.s.E = acc ? E : E0;
-  __syncthreads();
+  w.g.sync();
+  if (w.g.leader()) w.s.E = acc ? E : E0;
+  w.g.sync();
   return acc;
 }
 
@@ -533,12 +832,13 @@ __device__ inline bool cell_valid(const float* c, int n, const JrMoveParams& mv)
 
 // Volume move (volume.py:49-109 + _common.py:16-93).  Returns acceptance and
 // the reject reason (priority energy > cell > prior).
-__device__ bool move_volume(const JrParams& P, Walker& w, Key key, float step,
-                            double emax, float pressure, const float* mu,
-                            int& reason) {
+template <class G>
+__device__ __forceinline__ bool move_volume(const JrParams& P, Walker<G>& w, Key key, float step, double emax,
+                            float pressure, const float* mu, int& reason) {
   WalkShared& s = w.s;
   const WalkArrays& arr = w.arr;
   const int n = w.n;
+  const int r0 = w.g.rank(), gs = w.g.size();
   const JrMoveParams& mv = P.moves;
   const Key k1 = split(key, 0u), k2 = split(key, 1u);
   const int cur = s.cur, tr = cur ^ 1;
@@ -551,14 +851,15 @@ __device__ bool move_volume(const JrParams& P, Walker& w, Key key, float step,
   const float scale = __double2float_rn(pow((double)ratio, (double)(1.0f / 3.0f)));
   float nc[9];
   for (int q = 0; q < 9; ++q) nc[q] = __fmul_rn(h[q], scale);
-  if (threadIdx.x == 0) make_cell_ctx(nc, s.cc[tr], arr.T + tr * 3 * P.model.n_images, P.model);
   const int n3 = 3 * n;
-  for (int q = threadIdx.x; q < n3; q += blockDim.x) {
+  for (int q = r0; q < n3; q += gs) {
     float& x = pos_at(arr.xs, q);
     arr.x0[q] = x;
     x = __fmul_rn(x, scale);
   }
-  __syncthreads();
+  w.g.sync();
+  if (w.g.leader()) make_cell_ctx(nc, s.cc[tr], arr.T + tr * 3 * P.model.n_images, P.model);
+  w.g.sync();
   double d0, d1;
   const double En = ham_eval<false>(P, w, tr, pressure, mu, d0, d1);
   const bool valid = cell_valid(nc, n, mv);
@@ -586,19 +887,20 @@ __device__ bool move_volume(const JrParams& P, Walker& w, Key key, float step,
   const bool acc = energy_ok && valid && prior_ok;
   reason = acc ? 0 : (!energy_ok ? 1 : (!valid ? 2 : 3));
   if (!acc) {
-    for (int q = threadIdx.x; q < n3; q += blockDim.x) pos_at(arr.xs, q) = arr.x0[q];
+    for (int q = r0; q < n3; q += gs) pos_at(arr.xs, q) = arr.x0[q];
   }
-  __syncthreads();
-  if (threadIdx.x == 0 && acc) {
+  w.g.sync();
+  if (w.g.leader() && acc) {
     s.cur = tr;
     s.E = En;
   }
-  __syncthreads();
+  w.g.sync();
   return acc;
 }
 
 // alchemical_morph (alchemical.py:40-79).
-__device__ bool move_morph(const JrParams& P, Walker& w, Key key, double emax,
+template <class G>
+__device__ __forceinline__ bool move_morph(const JrParams& P, Walker<G>& w, Key key, double emax,
                            float pressure, const float* mu) {
   WalkShared& s = w.s;
   const WalkArrays& arr = w.arr;
@@ -606,18 +908,18 @@ __device__ bool move_morph(const JrParams& P, Walker& w, Key key, double emax,
   const int curt = __float_as_int(arr.xs[atom].w);
   const int cand = randint(split(key, 1u), 0, P.model.n_species - 1);
   const int nt = cand + (cand >= curt ? 1 : 0);
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  w.g.sync();
+  if (w.g.leader()) {
     arr.xs[atom].w = __int_as_float(nt);
     s.counts[curt] -= 1;
     s.counts[nt] += 1;
   }
-  __syncthreads();
+  w.g.sync();
   double d0, d1;
   const double En = ham_eval<false>(P, w, s.cur, pressure, mu, d0, d1);
   const bool acc = En < emax;
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  w.g.sync();
+  if (w.g.leader()) {
     if (acc) {
       s.E = En;
     } else {
@@ -626,13 +928,15 @@ __device__ bool move_morph(const JrParams& P, Walker& w, Key key, double emax,
       s.counts[nt] -= 1;
     }
   }
-  __syncthreads();
+  w.g.sync();
   return acc;
 }
 
 // species_swap over all species (swap.py:177-260).
-__device__ bool move_swap(const JrParams& P, Walker& w, Key key, double emax,
-                          float pressure, const float* mu) {
+template <class G>
+__device__ __forceinline__ bool move_swap(const JrParams& P, Walker<G>& w, Key key, double emax, float pressure,
+                          const float* mu) {
+  constexpr int kMaxPairs = JR_MAX_SPECIES * (JR_MAX_SPECIES - 1) / 2;
   WalkShared& s = w.s;
   const WalkArrays& arr = w.arr;
   const int n = w.n;
@@ -640,14 +944,14 @@ __device__ bool move_swap(const JrParams& P, Walker& w, Key key, double emax,
   const Key kp = split(key, 0u), klo = split(key, 1u), khi = split(key, 2u);
   int counts[JR_MAX_SPECIES];
   for (int q = 0; q < S; ++q) counts[q] = s.counts[q];
-  int plo[JR_MAX_SPECIES * JR_MAX_SPECIES], phi[JR_MAX_SPECIES * JR_MAX_SPECIES];
-  float cum[JR_MAX_SPECIES * JR_MAX_SPECIES];
+  uint8_t plo[kMaxPairs], phi[kMaxPairs];
+  float cum[kMaxPairs];
   int np = 0;
   float total = 0.0f;
   for (int a = 0; a < S; ++a)
     for (int b = a + 1; b < S; ++b) {
-      plo[np] = a;
-      phi[np] = b;
+      plo[np] = (uint8_t)a;
+      phi[np] = (uint8_t)b;
       total = __fadd_rn(total, (float)(counts[a] * counts[b]));
       cum[np] = total;
       ++np;
@@ -674,17 +978,17 @@ __device__ bool move_swap(const JrParams& P, Walker& w, Key key, double emax,
     }
   }
   const int tlo = __float_as_int(arr.xs[ilo].w), thi = __float_as_int(arr.xs[ihi].w);
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  w.g.sync();
+  if (w.g.leader()) {
     arr.xs[ilo].w = __int_as_float(chi);
     arr.xs[ihi].w = __int_as_float(clo);
   }
-  __syncthreads();
+  w.g.sync();
   double d0, d1;
   const double En = ham_eval<false>(P, w, s.cur, pressure, mu, d0, d1);
   const bool acc = (En < emax) && has_pair;
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  w.g.sync();
+  if (w.g.leader()) {
     if (acc) {
       s.E = En;
     } else {
@@ -692,20 +996,20 @@ __device__ bool move_swap(const JrParams& P, Walker& w, Key key, double emax,
       arr.xs[ihi].w = __int_as_float(thi);
     }
   }
-  __syncthreads();
+  w.g.sync();
   return acc;
 }
 
 // One move of type P.moves.type[idx]; returns acceptance and reject reason.
-__device__ __forceinline__ bool run_move(const JrParams& P, Walker& w, int idx,
-                                         Key key, float step, double emax,
-                                         float pressure, const float* mu,
-                                         int& reason) {
+template <class G>
+__device__ __forceinline__ bool run_move(const JrParams& P, Walker<G>& w, int idx, Key key,
+                                         float step, double emax, float pressure,
+                                         const float* mu, int& reason) {
   reason = 0;
   switch (P.moves.type[idx]) {
     case JR_MOVE_GALILEAN:
-      return move_galilean(P, w, key, step, P.moves.n_reflect[idx],
-                           P.moves.perturb_angle[idx], emax, pressure, mu);
+      return move_galilean(P, w, key, step, P.moves.n_reflect[idx], P.moves.perturb_angle[idx],
+                           emax, pressure, mu);
     case JR_MOVE_VOLUME:
       return move_volume(P, w, key, step, emax, pressure, mu, reason);
     case JR_MOVE_MORPH:
@@ -721,15 +1025,15 @@ __device__ __forceinline__ bool run_move(const JrParams& P, Walker& w, int idx,
 
 // MWG step (mwg.py:227-257 with the _wrap counters of mwg.py:108-150) plus
 // the ns_step scan-body counters (nested_sampling.py:541-609).
-__device__ __forceinline__ void mwg_step(const JrParams& P, Walker& w, Key step_key,
+template <class G>
+__device__ __forceinline__ void mwg_step(const JrParams& P, Walker<G>& w, Key step_key,
                                          Key move_key, double emax, float pressure,
                                          const float* mu) {
   WalkShared& s = w.s;
   const int idx = choice(move_key, P.moves.cum_probs, P.moves.n_moves);
   int reason = 0;
-  const bool acc = run_move(P, w, idx, step_key, s.step_sizes[idx], emax, pressure,
-                            mu, reason);
-  if (threadIdx.x == 0) {
+  const bool acc = run_move(P, w, idx, step_key, s.step_sizes[idx], emax, pressure, mu, reason);
+  if (w.g.leader()) {
     s.w_prop[idx] += 1;
     s.w_acc[idx] += acc ? 1 : 0;
     s.c_prop[idx] += 1;
@@ -745,35 +1049,41 @@ __device__ __forceinline__ void mwg_step(const JrParams& P, Walker& w, Key step_
 
 // ------------------------------------------------------ load / store ----
 
-__device__ inline void load_tables(const JrParams& P, WalkShared& s) {
+__device__ inline void load_tables(const JrParams& P, PairTables& t) {
   const int SS = P.model.n_species * P.model.n_species;
   for (int q = threadIdx.x; q < SS; q += blockDim.x) {
-    s.sig2[q] = P.model.sig2[q];
-    s.eps4[q] = P.model.eps4[q];
-    s.eps24[q] = P.model.eps24[q];
+    t.sig2[q] = P.model.sig2[q];
+    t.eps4[q] = P.model.eps4[q];
+    t.eps24[q] = P.model.eps24[q];
   }
 }
 
-// Load walker `slot` of replica p into smem.  zero_counters: a fresh clone
+// Load walker `slot` of replica p.  zero_counters: a fresh clone
 // (nested_sampling.py:507-512).
-__device__ inline void load_walker(const JrParams& P, const JrDims& D,
-                                   const JrStateBuffers& st, Walker& w, int p,
-                                   int slot, bool zero_counters) {
+template <class G>
+__device__ __forceinline__ void load_walker(const JrParams& P, const JrDims& D, const JrStateBuffers& st,
+                                   Walker<G>& w, int p, int slot, bool zero_counters) {
   WalkShared& s = w.s;
   const WalkArrays& arr = w.arr;
   const int n = w.n;
+  const int r0 = w.g.rank(), gs = w.g.size();
   const int K = D.n_walkers, Nmax = D.n_atoms_max, M = D.n_moves;
   const size_t wb = (size_t)p * K + slot;
   const float* gx = st.positions + wb * Nmax * 3;
   const float* gd = st.direction + wb * Nmax * 3;
   const int32_t* gt = st.types + wb * Nmax;
-  __syncthreads();
-  for (int q = threadIdx.x; q < 3 * n; q += blockDim.x) {
+  w.g.sync();
+  for (int q = r0; q < 3 * n; q += gs) {
     pos_at(arr.xs, q) = gx[q];
     arr.dir[q] = gd[q];
   }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) arr.xs[i].w = __int_as_float(gt[i]);
-  if (threadIdx.x == 0) {
+  const int smax = P.model.n_species - 1;
+  for (int i = r0; i < n; i += gs) {
+    // out-of-range species clamp like a JAX gather index
+    const int t = gt[i];
+    arr.xs[i].w = __int_as_float(t < 0 ? 0 : (t > smax ? smax : t));
+  }
+  if (w.g.leader()) {
     for (int q = 0; q < JR_MAX_SPECIES; ++q) s.counts[q] = 0;
     s.E = st.energy64[wb];
     for (int m = 0; m < M; ++m) {
@@ -784,30 +1094,32 @@ __device__ inline void load_walker(const JrParams& P, const JrDims& D,
     s.cur = 0;
     make_cell_ctx(st.cell + wb * 9, s.cc[0], arr.T, P.model);
   }
-  __syncthreads();
-  if (threadIdx.x == 0)
+  w.g.sync();
+  if (w.g.leader())
     for (int i = 0; i < n; ++i) s.counts[__float_as_int(arr.xs[i].w)] += 1;
-  __syncthreads();
+  w.g.sync();
 }
 
-// Store the smem walker into `slot` of replica p.
-__device__ inline void store_walker(const JrDims& D, const JrStateBuffers& st,
-                                    Walker& w, int p, int slot) {
+// Store the walker into `slot` of replica p.
+template <class G>
+__device__ __forceinline__ void store_walker(const JrDims& D, const JrStateBuffers& st, Walker<G>& w,
+                                    int p, int slot) {
   WalkShared& s = w.s;
   const WalkArrays& arr = w.arr;
   const int n = w.n;
+  const int r0 = w.g.rank(), gs = w.g.size();
   const int K = D.n_walkers, Nmax = D.n_atoms_max, M = D.n_moves;
   const size_t wb = (size_t)p * K + slot;
   float* gx = st.positions + wb * Nmax * 3;
   float* gd = st.direction + wb * Nmax * 3;
   int32_t* gt = st.types + wb * Nmax;
-  __syncthreads();
-  for (int q = threadIdx.x; q < 3 * n; q += blockDim.x) {
+  w.g.sync();
+  for (int q = r0; q < 3 * n; q += gs) {
     gx[q] = pos_at(arr.xs, q);
     gd[q] = arr.dir[q];
   }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) gt[i] = __float_as_int(arr.xs[i].w);
-  if (threadIdx.x == 0) {
+  for (int i = r0; i < n; i += gs) gt[i] = __float_as_int(arr.xs[i].w);
+  if (w.g.leader()) {
     st.energy64[wb] = s.E;
     st.energy[wb] = __double2float_rn(s.E);
     for (int q = 0; q < 9; ++q) st.cell[wb * 9 + q] = s.cc[s.cur].raw[q];
@@ -820,11 +1132,9 @@ __device__ inline void store_walker(const JrDims& D, const JrStateBuffers& st,
 }
 
 __device__ inline void zero_chain_counters(WalkShared& s) {
-  if (threadIdx.x == 0) {
-    for (int m = 0; m < JR_MAX_MOVES; ++m) {
-      s.c_acc[m] = s.c_prop[m] = s.c_nev[m] = s.c_ngr[m] = 0;
-      s.c_rr[4 * m] = s.c_rr[4 * m + 1] = s.c_rr[4 * m + 2] = s.c_rr[4 * m + 3] = 0;
-    }
+  for (int m = 0; m < JR_MAX_MOVES; ++m) {
+    s.c_acc[m] = s.c_prop[m] = s.c_nev[m] = s.c_ngr[m] = 0;
+    s.c_rr[4 * m] = s.c_rr[4 * m + 1] = s.c_rr[4 * m + 2] = s.c_rr[4 * m + 3] = 0;
   }
 }
 

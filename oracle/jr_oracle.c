@@ -262,6 +262,22 @@ static int center_image(const JroModel* m) {
   return -1;
 }
 
+/* Kernel reciprocal: bit-pattern seed + three FMA Newton-Raphson steps
+ * (max 0.501 ulp); outside [2^-120, 2^120] the correctly rounded 1/x. */
+static inline float rcp_nr(float x) {
+  if (!(x >= 0x1p-120f && x <= 0x1p120f)) return 1.0f / x;
+  uint32_t u;
+  memcpy(&u, &x, 4);
+  u = 0x7EF311C3u - u;
+  float y;
+  memcpy(&y, &u, 4);
+  for (int k = 0; k < 3; ++k) {
+    float e = fmaf(-x, y, 1.0f);
+    y = fmaf(y, e, y);
+  }
+  return y;
+}
+
 /* DEV contract, one ordered pair: r2 by FMA chain, reciprocal, LJ powers. */
 static inline void dev_pair(const JroModel* m, int ti, int tj, float dx,
                             float dy, float dz, float* e, float* g) {
@@ -277,7 +293,7 @@ static inline void dev_pair(const JroModel* m, int ti, int tj, float dx,
   float sig2 = m->sig2[ti * S + tj];
   float eps4 = m->eps4[ti * S + tj];
   float eps24 = m->eps24[ti * S + tj];
-  float ri = 1.0f / r2;
+  float ri = rcp_nr(r2);
   float s2 = sig2 * ri;
   float s4 = s2 * s2;
   float s6 = s4 * s2;
@@ -312,43 +328,61 @@ static double lj_dev(const JroModel* m, int n, const float* x,
       T[3 * k + q] = v;
     }
   }
+  /* Energy: float64 sum of the float32 pair terms.  Forces: float32 in the
+   * canonical order -- partners in blocks of 8 (ascending j, then image),
+   * block partials combined pairwise over L = next_pow2(ceil(n/8)) slots. */
+  int nb = (n + 7) / 8, L = 1;
+  while (L < nb) L <<= 1;
   double E = 0.0;
   for (int i = 0; i < n; ++i) {
-    double fi[3] = {0.0, 0.0, 0.0};
-    for (int j = 0; j < n; ++j) {
-      float dr[3], d[3];
-      for (int q = 0; q < 3; ++q) dr[q] = x[3 * j + q] - x[3 * i + q];
-      float nn[3];
-      for (int q = 0; q < 3; ++q) {
-        float f = dr[0] * inv[q];
-        f = fmaf(dr[1], inv[3 + q], f);
-        f = fmaf(dr[2], inv[6 + q], f);
-        nn[q] = rintf(f);
-      }
-      for (int q = 0; q < 3; ++q) {
-        float s = nn[0] * c[q];
-        s = fmaf(nn[1], c[3 + q], s);
-        s = fmaf(nn[2], c[6 + q], s);
-        d[q] = dr[q] - s;
-      }
-      for (int k = 0; k < nimg; ++k) {
-        if (k == ctr && i == j) continue;
-        float dd[3];
-        if (nimg > 1) {
-          for (int q = 0; q < 3; ++q) dd[q] = d[q] + T[3 * k + q];
-        } else {
-          dd[0] = d[0]; dd[1] = d[1]; dd[2] = d[2];
+    float Pb[32][3];
+    memset(Pb, 0, sizeof(Pb));
+    for (int b = 0; b < L; ++b) {
+      const int j0 = 8 * b, j1 = j0 + 8 < n ? j0 + 8 : n;
+      for (int j = j0; j < j1; ++j) {
+        float dr[3], d[3];
+        for (int q = 0; q < 3; ++q) dr[q] = x[3 * j + q] - x[3 * i + q];
+        float nn[3];
+        for (int q = 0; q < 3; ++q) {
+          float f = dr[0] * inv[q];
+          f = fmaf(dr[1], inv[3 + q], f);
+          f = fmaf(dr[2], inv[6 + q], f);
+          nn[q] = rintf(f);
         }
-        float e, g;
-        dev_pair(m, t[i], t[j], dd[0], dd[1], dd[2], &e, &g);
-        E += (double)e;
-        if (F && i != j) {
-          for (int q = 0; q < 3; ++q) fi[q] += (double)(g * dd[q]);
+        for (int q = 0; q < 3; ++q) {
+          float s = nn[0] * c[q];
+          s = fmaf(nn[1], c[3 + q], s);
+          s = fmaf(nn[2], c[6 + q], s);
+          d[q] = dr[q] - s;
+        }
+        for (int k = 0; k < nimg; ++k) {
+          if (k == ctr && i == j) continue;
+          float dd[3];
+          if (nimg > 1) {
+            for (int q = 0; q < 3; ++q) dd[q] = d[q] + T[3 * k + q];
+          } else {
+            dd[0] = d[0]; dd[1] = d[1]; dd[2] = d[2];
+          }
+          float e, g;
+          dev_pair(m, t[i], t[j], dd[0], dd[1], dd[2], &e, &g);
+          E += (double)e;
+          if (F && i != j)
+            for (int q = 0; q < 3; ++q) {
+              float term = g * dd[q];
+              Pb[b][q] = Pb[b][q] + term;
+            }
         }
       }
     }
-    if (F)
-      for (int q = 0; q < 3; ++q) F[3 * i + q] = (double)(float)fi[q];
+    if (F) {
+      for (int s = 1; s < L; s <<= 1) {
+        float Q[32][3];
+        for (int b = 0; b < L; ++b)
+          for (int q = 0; q < 3; ++q) Q[b][q] = Pb[b][q] + Pb[b ^ s][q];
+        memcpy(Pb, Q, sizeof(float) * 3 * L);
+      }
+      for (int q = 0; q < 3; ++q) F[3 * i + q] = (double)Pb[0][q];
+    }
   }
   return 0.5 * E;
 }
@@ -630,9 +664,9 @@ static int move_galilean(const JroModel* mdl, int mode, const uint32_t key[2],
           sff += (double)Ff[i] * (double)Ff[i];
           sfd += (double)Ff[i] * (double)v[i];
         }
-        double nrm = sqrt(sff);
-        if (nrm < 1e-10) nrm = 1e-10;
-        float coef = (float)(2.0 * sfd / (nrm * nrm));
+        /* coefficient 2 (F.d) / max(|F|^2, 1e-20) with the scalar in float32 */
+        float ffs = (float)sff;
+        float coef = (2.0f * (float)sfd) * rcp_nr(ffs > 1e-20f ? ffs : 1e-20f);
         for (int i = 0; i < n3; ++i) v[i] = fmaf(-coef, Ff[i], v[i]);
       }
     }

@@ -1,0 +1,193 @@
+"""Host-side logic and the C ABI boundary (CPU only, no compute calls)."""
+
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from jaxrens_b200 import _lib, create_lj, prior_mass, prng
+from jaxrens_b200 import moves as mvs
+from jaxrens_b200 import nested_sampling as nsm
+from jaxrens_b200.backends import EnsembleTerm, Hamiltonian, make_image_offsets
+from jaxrens_b200.mwg import build_mwg
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "jaxrens_b200.h")
+
+
+def _declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(jr_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    from jaxrens_b200 import _build
+
+    _build.build()
+    L = C.CDLL(_lib.LIB_PATH)
+    declared = _declared_functions()
+    assert sorted(_lib.EXPORTED) == declared
+    for name in declared:
+        assert hasattr(L, name), name
+    assert _lib.load().jr_version() >= 2
+
+
+def test_struct_layout_matches_header():
+    prog = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "jaxrens_b200.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(JrDims), sizeof(JrModelParams),
+         sizeof(JrMoveParams), sizeof(JrParams), sizeof(JrStateBuffers), sizeof(JrInfoBuffers),
+         sizeof(JrLaunchConfig), offsetof(JrParams, log_alpha), offsetof(JrModelParams, gm_sigma));
+  return 0;
+}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        open(c, "w").write(prog)
+        exe = os.path.join(d, "t")
+        subprocess.run(["gcc", "-I", os.path.dirname(HEADER), c, "-o", exe], check=True)
+        got = [int(v) for v in subprocess.run([exe], capture_output=True, text=True,
+                                              check=True).stdout.split()]
+    want = [C.sizeof(_lib.JrDims), C.sizeof(_lib.JrModelParams), C.sizeof(_lib.JrMoveParams),
+            C.sizeof(_lib.JrParams), C.sizeof(_lib.JrStateBuffers), C.sizeof(_lib.JrInfoBuffers),
+            C.sizeof(_lib.JrLaunchConfig), _lib.JrParams.log_alpha.offset,
+            _lib.JrModelParams.gm_sigma.offset]
+    assert got == want
+
+
+def test_invalid_arguments_fail_loudly_without_a_gpu():
+    L = _lib.load()
+    d = _lib.JrDims(1, 16, 8, 2, 4, 0, 2, 0)  # n_cull = 2 is outside this build
+    p = _lib.JrParams()
+    p.model.n_species = 1
+    p.model.n_images = 1
+    p.moves.n_moves = 2
+    rc = L.jr_ns_iterate(C.byref(d), C.byref(p), C.byref(_lib.JrStateBuffers()), None, 1,
+                         None, None, 0, None)
+    assert rc == -6
+    assert b"n_cull" in L.jr_last_error()
+    with pytest.raises(_lib.JrError):
+        _lib.check(rc, "jr_ns_iterate")
+
+
+def test_lj_tables_follow_reference_rounding():
+    a = create_lj(epsilon=0.7, sigma=0.9, cutoff=2.5)
+    assert a.eps4[0, 0] == np.float32(4.0 * 0.7)
+    assert a.sig2[0, 0] == np.float32(0.9 * 0.9)
+    b = create_lj(epsilon=[0.7, 0.7], sigma=[0.9, 0.9])
+    # the table path squares the float32 sigma (lj.py:186) -- may differ by 1 ulp
+    assert abs(float(b.sig2[0, 1]) - 0.81) < 1e-6
+    lb = create_lj(epsilon=[1.0, 0.5], sigma=[1.0, 1.2])
+    assert lb.eps4[0, 1] == np.float32(4.0) * np.sqrt(np.float32(1.0) * np.float32(0.5))
+    assert lb.sig2[0, 1] == np.float32(1.1) * np.float32(1.1)
+    with pytest.raises(ValueError):
+        create_lj(epsilon=[1.0, 1.0], sigma=1.0)
+    with pytest.raises(ValueError):
+        create_lj(supercell_trafo=(0, 1, 1))
+
+
+def test_image_offsets_like_reference():
+    assert make_image_offsets(1, 1, 1).tolist() == [[0, 0, 0]]
+    assert len(make_image_offsets(2, 2, 2)) == 27
+    assert len(make_image_offsets(4, 4, 4)) == 125
+
+
+def test_build_mwg_probabilities_and_params():
+    H = Hamiltonian(create_lj(cutoff=2.5), [EnsembleTerm(pressure=0.1)])
+    _, step, per = build_mwg(H, [mvs.gmc(n_reflect=10, weight=4.0), mvs.volume_move(32)])
+    assert step.params.moves.n_moves == 2
+    assert np.float32(step.params.moves.cum_probs[0]) == np.float32(0.8)
+    assert np.float32(step.params.moves.cum_probs[1]) == np.float32(1.0)
+    assert step.params.moves.n_reflect[0] == 10
+    assert len(per) == 2
+    with pytest.raises(NotImplementedError):
+        build_mwg(H, [mvs.MoveKernel("g", mvs.galilean.build_kernel,
+                                     kernel_kwargs={"use_forces": False})])
+
+
+def test_re_firing_schedule_and_key_chain():
+    re = nsm.InterREManager(10, 1, prng.key(5))
+    assert [i for i in range(35) if re.fires(i)] == [10, 20, 30]
+    k0 = re.key.copy()
+    sk = re.next_swap_key()
+    a, b = prng.split(k0, 2)
+    assert np.array_equal(re.key, a)
+    assert np.array_equal(sk, prng.split(b, 2)[1])
+
+
+def test_prior_mass_termination_semantics():
+    t = nsm.PriorMassTermination(n_live=32, threshold=1e-3)
+    assert not t.check(10, 5.0)  # never before every walker was replaced once
+    t.update_evidence(-2.0)
+    la = prior_mass.log_alpha(32, 1)
+    it = 5000
+    assert t.check(it, -((it + 1) * la) + 2.0 + 10.0) is True
+    assert nsm.IterationTermination(100).check(99, 0.0)
+
+
+def test_oracle_ns_step_counter_invariants_and_evidence():
+    from tests._cases import lj_case, oracle_replicas
+
+    case = lj_case(P=1, K=24, N=8, seed=12, n_reflect=3, T=6)
+    rep = oracle_replicas(case)[0]
+    la = prior_mass.log_alpha(24, 1)
+    wo = float(prior_mass.iteration_offsets(24, 1)[1][0])
+    last = -np.inf
+    emaxes = []
+    for _ in range(40):
+        info, *_ = O.ns_step(case["model"], case["moves"], rep, 6, la, wo)
+        for m in range(2):
+            assert info.rr[4 * m] == info.n_acc[m]
+            assert sum(info.rr[4 * m: 4 * m + 4]) == info.n_prop[m]
+        assert sum(info.n_prop[:2]) == 6
+        assert rep.log_evidence[0] >= last
+        last = rep.log_evidence[0]
+        emaxes.append(info.emax)
+        assert rep.energy.max() <= info.emax
+    assert all(b <= a for a, b in zip(emaxes, emaxes[1:]))
+
+
+def test_worst_walker_ties_break_on_noise():
+    from tests._cases import lj_case, oracle_replicas
+
+    case = lj_case(P=1, K=16, N=4, seed=13, n_reflect=2, T=1)
+    rep = oracle_replicas(case)[0]
+    rep.energy[:] = 7.0
+    key = rep.rng_key.copy()
+    info, *_ = O.ns_step(case["model"], case["moves"], rep, 1, prior_mass.log_alpha(16, 1),
+                         float(prior_mass.iteration_offsets(16, 1)[1][0]))
+    kw = prng.split(key, 2)[1]
+    assert info.worst_idx == int(np.argmax(prng.uniform(kw, 16)))
+
+
+def test_oracle_replica_exchange_keeps_energies_in_receiving_frame():
+    from tests._cases import lj_case, oracle_replicas
+
+    case = lj_case(P=4, K=12, N=6, seed=14, n_reflect=2, T=2,
+                   pressure=np.array([0.01, 0.1, 0.5, 1.0]))
+    reps = oracle_replicas(case)
+    for r in reps:
+        r.emax[0] = np.inf
+    acc, att = O.re_step(reps, prng.key(3), n_swap_cycles=3)
+    assert att.sum() == 3 * 3 and acc.sum() > 0
+    for r in reps:
+        for k in range(12):
+            e = O.energy(case["model"], r.positions[k], r.types[k], r.cell[k],
+                         pressure=r.pressure, forces=False)[0]
+            assert abs(e - r.energy[k]) <= 1e-9 * max(1.0, abs(e))
+
+
+def test_host_prng_matches_oracle():
+    k = prng.key(77)
+    assert np.array_equal(prng.split(k, 9), O.split(k, 9))
+    assert np.array_equal(prng.fold_in(k, 1), O.fold_in(k, 1))
+    assert np.array_equal(prng.advance_iteration(k), O.split(O.split(k, 2)[0], 5)[0])
