@@ -716,6 +716,40 @@ JrLaunchConfig heuristic_config(const JrDims* d) {
   return c;
 }
 
+// Speculation depth bound of check_config, without setting the error text.
+bool spec_fits(const JrLaunchConfig& c, const JrDims* d) {
+  const int W = 1 + d->n_extra;
+  const int slots = c.cluster * (c.warp_walkers ? c.threads / 32 : 1);
+  if (slots < 2 * W) return true;
+  const int D = slots / W < jr::kMaxD ? slots / W : jr::kMaxD;
+  return D * d->n_extra <= jr::kMaxWalk && D * W <= jr::kMaxWalk;
+}
+
+// Default shape of the NS launch: a CTA per walker chain (256 threads) for
+// 16 < N <= 64, warp walkers for N <= 16, and the largest power-of-two
+// cluster (<= 16) that keeps one CTA per replica-cluster member on every SM.
+JrLaunchConfig ns_heuristic_config(const JrDims* d) {
+  JrLaunchConfig c = heuristic_config(d);
+  const int nmax = d->n_atoms_max;
+  if (nmax > 16 && nmax <= 64) {
+    c.warp_walkers = 0;
+    c.threads = 256;
+    const int tpa = pow2_floor(c.threads / nmax);
+    c.tpa = tpa > 16 ? 16 : (tpa < 1 ? 1 : tpa);
+  }
+  int sms = 148, dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    sms = 148;
+  }
+  int cl = 1;
+  while (cl * 2 <= 16 && d->n_replicas * cl * 2 <= sms) cl *= 2;
+  c.cluster = cl;
+  while (c.cluster > 1 && !spec_fits(c, d)) c.cluster /= 2;
+  return c;
+}
+
 int check_params(const JrDims* d, const JrParams* p) {
   if (!d || !p) return fail(JR_ERR_PARAM, "null dims or params");
   if (d->n_replicas < 1 || d->n_walkers < 2 || d->n_atoms_max < 1 ||
@@ -833,7 +867,7 @@ int jr_ns_iterate(const JrDims* dims, const JrParams* params, const JrStateBuffe
   } else {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(tune_key(dims, params));
-    c = it != g_tune_cache.end() ? it->second : heuristic_config(dims);
+    c = it != g_tune_cache.end() ? it->second : ns_heuristic_config(dims);
   }
   rc = check_config(c, dims);
   if (rc) return rc;
@@ -1027,7 +1061,7 @@ extern "C" int jr_autotune(const JrDims* dims, const JrParams* params,
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   float best_ms = 1e30f;
-  JrLaunchConfig bc = heuristic_config(dims);
+  JrLaunchConfig bc = ns_heuristic_config(dims);
   const int nmax = dims->n_atoms_max;
   JrLaunchConfig cands[96];
   int nc = 0;
