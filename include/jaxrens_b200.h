@@ -177,6 +177,21 @@ int jr_ns_iterate(const JrDims* dims, const JrParams* params,
                   int32_t n_iter, const JrLaunchConfig* cfg, void* workspace,
                   size_t workspace_bytes, void* stream);
 
+/* jr_ns_iterate for callers that cannot allocate device memory (an XLA FFI
+ * handler given no scratch operand, a host that forbids allocation after
+ * start-up).  It has no counterpart in the reference.  Instead of a caller
+ * workspace it uses a 256-byte static __device__ array inside this library;
+ * dims whose jr_ns_iterate_workspace_size() exceeds 256 bytes are rejected
+ * with JR_ERR_WORKSPACE.  It allocates nothing.  The first call on each
+ * device resolves that array's address (cudaGetSymbolAddress, device
+ * current) and caches it, so make that first call before any stream capture.
+ * The scratch is shared by every call on a device: calls that overlap in
+ * time (several host threads, or concurrent streams) race on it and must be
+ * serialised by the caller. */
+int jr_ns_iterate_static(const JrDims* dims, const JrParams* params,
+                         const JrStateBuffers* state, const JrInfoBuffers* info,
+                         int32_t n_iter, const JrLaunchConfig* cfg, void* stream);
+
 /* ---- one move per (replica, trial) walker (adaptation / burn-in) ---- */
 /* walker_idx [P][n_trials], keys [P][n_trials][2], step [P], emax [P];
  * accepted [P][n_trials].  write_back=1 stores the moved walkers in place

@@ -132,6 +132,7 @@ class JrLaunchConfig(C.Structure):
 EXPORTED = (
     "jr_ns_iterate_workspace_size",
     "jr_ns_iterate",
+    "jr_ns_iterate_static",
     "jr_move_trial",
     "jr_energy_forces",
     "jr_re_swap",
@@ -175,6 +176,11 @@ def load():
     L.jr_ns_iterate.argtypes = [
         P(JrDims), P(JrParams), P(JrStateBuffers), P(JrInfoBuffers), C.c_int32,
         P(JrLaunchConfig), _vp, C.c_size_t, _vp,
+    ]
+    L.jr_ns_iterate_static.restype = C.c_int
+    L.jr_ns_iterate_static.argtypes = [
+        P(JrDims), P(JrParams), P(JrStateBuffers), P(JrInfoBuffers), C.c_int32,
+        P(JrLaunchConfig), _vp,
     ]
     L.jr_move_trial.restype = C.c_int
     L.jr_move_trial.argtypes = [

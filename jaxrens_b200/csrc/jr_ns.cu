@@ -883,6 +883,52 @@ int jr_ns_iterate(const JrDims* dims, const JrParams* params, const JrStateBuffe
   return launch_ns<jr::CtaGroup>(dims, params, state, inf, n_iter, c, workspace, s);
 }
 
+}  // extern "C"
+
+// Scratch of jr_ns_iterate_static: the same bytes jr_ns_iterate keeps in the
+// caller's workspace (the snapshot of replica 0's key, rewritten by every call
+// before its launch, so nothing in it has to start at zero).
+static constexpr size_t kStaticScratchBytes = 256;
+static constexpr int kMaxStaticDevices = 64;
+static __device__ __align__(256) unsigned char jr_static_scratch[kStaticScratchBytes];
+static std::mutex g_static_mu;
+static void* g_static_ptr[kMaxStaticDevices];
+
+extern "C" {
+
+// jr_ns_iterate on the library's own static device scratch instead of a
+// caller workspace.  The first call on each device resolves the scratch's
+// address with cudaGetSymbolAddress (with that device current) and caches it.
+int jr_ns_iterate_static(const JrDims* dims, const JrParams* params,
+                         const JrStateBuffers* state, const JrInfoBuffers* info, int32_t n_iter,
+                         const JrLaunchConfig* cfg, void* stream) {
+  int rc = check_params(dims, params);
+  if (rc) return rc;
+  const size_t need = jr_ns_iterate_workspace_size(dims);
+  if (need > kStaticScratchBytes)
+    return fail(JR_ERR_WORKSPACE, "jr_ns_iterate_static: these dims need " +
+                                      std::to_string(need) + " bytes of scratch; the static "
+                                      "scratch holds " + std::to_string(kStaticScratchBytes));
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "jr_ns_iterate_static: cudaGetDevice");
+  if (dev < 0 || dev >= kMaxStaticDevices)
+    return fail(JR_ERR_PARAM, "jr_ns_iterate_static: device ordinal beyond 63");
+  void* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    scratch = g_static_ptr[dev];
+    if (!scratch) {
+      e = cudaGetSymbolAddress(&scratch, jr_static_scratch);
+      if (e != cudaSuccess)
+        return cuda_fail(e, "jr_ns_iterate_static: cudaGetSymbolAddress of the static scratch");
+      g_static_ptr[dev] = scratch;
+    }
+  }
+  return jr_ns_iterate(dims, params, state, info, n_iter, cfg, scratch, kStaticScratchBytes,
+                       stream);
+}
+
 int jr_move_trial(const JrDims* dims, const JrParams* params, const JrStateBuffers* state,
                   int32_t n_trials, int32_t move_idx, const int32_t* walker_idx,
                   const uint32_t* keys, const uint32_t* move_keys, const float* step,
