@@ -564,26 +564,32 @@ energy_kernel(const JrParams Pg, const int n_configs, const int nmax, const floa
 
 // --------------------------------------------------------- RE swaps ----
 // Ensemble term of walker (p_conf, slot) under replica p_ens's parameters.
+// P*V - mu.N of the walker at (p_conf, slot) under run p_ens's ensemble, one
+// warp: lanes count the species, every lane returns the same value.
 __device__ double walker_ens(const JrDims& D, const JrStateBuffers& st, int p_conf, int slot,
-                             int p_ens, int S) {
+                             int p_ens, int S, int lane) {
   const int K = D.n_walkers, Nmax = D.n_atoms_max;
   const size_t wb = (size_t)p_conf * K + slot;
   const float vol = fabsf(det3(st.cell + wb * 9));
   double e = (double)st.pressure[p_ens] * (double)vol;
   if (st.mu) {
-    int counts[JR_MAX_SPECIES] = {0};
     const int n = min(max(st.n_atoms[p_conf], 1), Nmax);
-    for (int i = 0; i < n; ++i) counts[min(max(st.types[wb * Nmax + i], 0), S - 1)]++;
     double dot = 0.0;
-    for (int q = 0; q < S; ++q) dot += (double)st.mu[(size_t)p_ens * S + q] * (double)counts[q];
+    for (int q = 0; q < S; ++q) {
+      int c = 0;
+      for (int i = lane; i < n; i += 32)
+        c += min(max(st.types[wb * Nmax + i], 0), S - 1) == q ? 1 : 0;
+      c = __reduce_add_sync(0xffffffffu, c);
+      dot += (double)st.mu[(size_t)p_ens * S + q] * (double)c;
+    }
     e = e - dot;
   }
   return e;
 }
 
 template <typename Tp>
-__device__ void swap_range(Tp* a, Tp* b, int n) {
-  for (int q = 0; q < n; ++q) {
+__device__ void swap_range(Tp* a, Tp* b, int n, int lane) {
+  for (int q = lane; q < n; q += 32) {
     Tp t = a[q];
     a[q] = b[q];
     b[q] = t;
@@ -591,47 +597,56 @@ __device__ void swap_range(Tp* a, Tp* b, int n) {
 }
 
 // replica_exchange_step with EnsembleSwap (replica_exchange.py:318-436).
+// One CTA; within a phase the pairs touch disjoint runs, so warp w serves
+// pair slots w, w + nwarps, ...; phases and cycles are separated by a CTA
+// barrier because each one sees the swaps of the one before.
 __global__ void re_swap_kernel(const JrDims D, const JrStateBuffers st, const Key key,
                                const int n_cycles, const int S, int* acc_pp, int* att_pp) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int R = D.n_replicas, K = D.n_walkers, Nmax = D.n_atoms_max;
   const int n_even = R / 2, n_odd = (R - 1) / 2;
   const int max_pairs = n_even > n_odd ? n_even : n_odd;
-  for (int q = 0; q < R - 1; ++q) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int q = threadIdx.x; q < R - 1; q += blockDim.x) {
     if (acc_pp) acc_pp[q] = 0;
     if (att_pp) att_pp[q] = 0;
   }
+  __syncthreads();
   for (int cyc = 0; cyc < n_cycles; ++cyc) {
     const Key ck = split(key, (uint32_t)cyc);
     for (int phase = 0; phase < 2; ++phase) {
       const Key pk = split(ck, (uint32_t)phase);
       const int nv = phase == 0 ? n_even : n_odd;
-      for (int slot = 0; slot < max_pairs; ++slot) {
+      for (int slot = warp; slot < max_pairs && slot < nv; slot += nwarps) {
         const Key sk = split(pk, (uint32_t)slot);
         const int wi = randint(split(sk, 0u), 0, K);
         const int wj = randint(split(sk, 1u), 0, K);
-        if (slot >= nv) continue;
         const int ri = phase + 2 * slot, rj = ri + 1;
         const size_t bi = (size_t)ri * K + wi, bj = (size_t)rj * K + wj;
         // into_i: walker j re-expressed in run i's ensemble (ensemble.py:62-87)
-        const double into_i =
-            (st.energy64[bj] - walker_ens(D, st, rj, wj, rj, S)) + walker_ens(D, st, rj, wj, ri, S);
-        const double into_j =
-            (st.energy64[bi] - walker_ens(D, st, ri, wi, ri, S)) + walker_ens(D, st, ri, wi, rj, S);
+        const double ej = st.energy64[bj], ei = st.energy64[bi];
+        const double into_i = (ej - walker_ens(D, st, rj, wj, rj, S, lane)) +
+                              walker_ens(D, st, rj, wj, ri, S, lane);
+        const double into_j = (ei - walker_ens(D, st, ri, wi, ri, S, lane)) +
+                              walker_ens(D, st, ri, wi, rj, S, lane);
         const bool do_swap = (into_i < st.emax[ri]) && (into_j < st.emax[rj]);
         if (do_swap) {
-          swap_range(st.positions + bi * Nmax * 3, st.positions + bj * Nmax * 3, Nmax * 3);
-          swap_range(st.direction + bi * Nmax * 3, st.direction + bj * Nmax * 3, Nmax * 3);
-          swap_range(st.types + bi * Nmax, st.types + bj * Nmax, Nmax);
-          swap_range(st.cell + bi * 9, st.cell + bj * 9, 9);
-          st.energy64[bi] = into_i;
-          st.energy64[bj] = into_j;
-          st.energy[bi] = __double2float_rn(into_i);
-          st.energy[bj] = __double2float_rn(into_j);
+          swap_range(st.positions + bi * Nmax * 3, st.positions + bj * Nmax * 3, Nmax * 3, lane);
+          swap_range(st.direction + bi * Nmax * 3, st.direction + bj * Nmax * 3, Nmax * 3, lane);
+          swap_range(st.types + bi * Nmax, st.types + bj * Nmax, Nmax, lane);
+          swap_range(st.cell + bi * 9, st.cell + bj * 9, 9, lane);
+          if (lane == 0) {
+            st.energy64[bi] = into_i;
+            st.energy64[bj] = into_j;
+            st.energy[bi] = __double2float_rn(into_i);
+            st.energy[bj] = __double2float_rn(into_j);
+          }
         }
-        if (acc_pp) acc_pp[ri] += do_swap ? 1 : 0;
-        if (att_pp) att_pp[ri] += 1;
+        if (lane == 0) {
+          if (acc_pp) acc_pp[ri] += do_swap ? 1 : 0;
+          if (att_pp) att_pp[ri] += 1;
+        }
       }
+      __syncthreads();
     }
   }
 }
@@ -703,7 +718,7 @@ JrLaunchConfig heuristic_config(const JrDims* d) {
   JrLaunchConfig c;
   const int nmax = d->n_atoms_max;
   c.cluster = 1;
-  if (nmax <= 64) {
+  if (nmax <= 32) {
     c.warp_walkers = 1;
     c.threads = 128;
     c.tpa = warp_tpa(nmax);
@@ -726,9 +741,12 @@ bool spec_fits(const JrLaunchConfig& c, const JrDims* d) {
 }
 
 // Default shape of the NS launch: a CTA per walker chain (256 threads) for
-// 16 < N <= 64, warp walkers for N <= 16, and the largest power-of-two
-// cluster (<= 16) that keeps one CTA per replica-cluster member on every SM.
-JrLaunchConfig ns_heuristic_config(const JrDims* d) {
+// 16 < N <= 64, warp walkers for N <= 16.  The cluster serves the speculative
+// iterations of one run: no more CTAs than one launch's n_iter * (1 + n_extra)
+// chains can use, at most 10 (larger clusters were measured to share SMs
+// between their CTAs, which slows every chain), and a grid under about 55% of
+// the SMs for the same reason.
+JrLaunchConfig ns_heuristic_config(const JrDims* d, int n_iter) {
   JrLaunchConfig c = heuristic_config(d);
   const int nmax = d->n_atoms_max;
   if (nmax > 16 && nmax <= 64) {
@@ -743,10 +761,16 @@ JrLaunchConfig ns_heuristic_config(const JrDims* d) {
     cudaGetLastError();
     sms = 148;
   }
-  int cl = 1;
-  while (cl * 2 <= 16 && d->n_replicas * cl * 2 <= sms) cl *= 2;
+  const int W = 1 + d->n_extra;
+  const int cpc = c.warp_walkers ? c.threads / 32 : 1;
+  const int want = (n_iter > 0 ? n_iter : 1) * W;              // chains one launch can use
+  int cl = (want + cpc - 1) / cpc;
+  const int fit = (sms * 11 / 20) / (d->n_replicas > 0 ? d->n_replicas : 1);
+  if (cl > 10) cl = 10;
+  if (cl > fit) cl = fit;
+  if (cl < 1) cl = 1;
   c.cluster = cl;
-  while (c.cluster > 1 && !spec_fits(c, d)) c.cluster /= 2;
+  while (c.cluster > 1 && !spec_fits(c, d)) c.cluster -= 1;
   return c;
 }
 
@@ -867,7 +891,7 @@ int jr_ns_iterate(const JrDims* dims, const JrParams* params, const JrStateBuffe
   } else {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(tune_key(dims, params));
-    c = it != g_tune_cache.end() ? it->second : ns_heuristic_config(dims);
+    c = it != g_tune_cache.end() ? it->second : ns_heuristic_config(dims, n_iter);
   }
   rc = check_config(c, dims);
   if (rc) return rc;
@@ -1014,7 +1038,9 @@ int jr_re_swap(const JrDims* dims, const JrStateBuffers* state, uint32_t key0, u
   if (n_swap_cycles < 0 || n_species < 1 || n_species > JR_MAX_SPECIES)
     return fail(JR_ERR_PARAM, "invalid swap parameters");
   if (dims->n_replicas < 2) return JR_OK;
-  jr::re_swap_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(*dims, *state, jr::Key{key0, key1},
+  const int max_pairs = dims->n_replicas / 2;  // even-phase pairs, >= the odd ones
+  const int warps = max_pairs < 1 ? 1 : (max_pairs > 32 ? 32 : max_pairs);
+  jr::re_swap_kernel<<<1, 32 * warps, 0, (cudaStream_t)stream>>>(*dims, *state, jr::Key{key0, key1},
                                                         n_swap_cycles, n_species, acc_per_pair,
                                                         att_per_pair);
   cudaError_t e = cudaGetLastError();
@@ -1107,12 +1133,12 @@ extern "C" int jr_autotune(const JrDims* dims, const JrParams* params,
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   float best_ms = 1e30f;
-  JrLaunchConfig bc = ns_heuristic_config(dims);
+  JrLaunchConfig bc = ns_heuristic_config(dims, n_iter_probe);
   const int nmax = dims->n_atoms_max;
   JrLaunchConfig cands[96];
   int nc = 0;
-  const int clusters[] = {1, 2, 4, 8, 12, 16};
-  if (nmax <= 64) {  // warp walkers: 1..8 walkers per CTA
+  const int clusters[] = {1, 2, 4, 8, 10, 12, 16};
+  if (nmax <= 32) {  // warp walkers: 1..8 walkers per CTA
     for (int wpc : {1, 2, 4})
       for (int cl : clusters) cands[nc++] = JrLaunchConfig{32 * wpc, warp_tpa(nmax), cl, 1};
   }

@@ -20,7 +20,7 @@
 namespace jr {
 
 constexpr int kMaxWarps = 32;
-constexpr int kPairMatMax = 128;  // walkers up to this size use the pair buffer
+constexpr int kPairMatMax = 64;  // walkers up to this size use the pair matrix
 
 // ------------------------------------------------------------- groups ----
 
@@ -49,14 +49,19 @@ struct CtaGroup {
       buf[warp][2] = c;
     }
     __syncthreads();
-    a = 0.0;
-    b = 0.0;
-    c = 0.0;
-    for (int q = 0; q < nw; ++q) {
-      a += buf[q][0];
-      b += buf[q][1];
-      c += buf[q][2];
+    // lane q < nw takes warp q's partials (zero above); a butterfly over the
+    // lowest next_pow2(nw) lanes puts the totals in lane 0, which broadcasts
+    a = lane < nw ? buf[lane][0] : 0.0;
+    b = lane < nw ? buf[lane][1] : 0.0;
+    c = lane < nw ? buf[lane][2] : 0.0;
+    for (int off = 1; off < nw; off <<= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, off);
+      b += __shfl_xor_sync(0xffffffffu, b, off);
+      c += __shfl_xor_sync(0xffffffffu, c, off);
     }
+    a = __shfl_sync(0xffffffffu, a, 0);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    c = __shfl_sync(0xffffffffu, c, 0);
     par ^= 1;
   }
 };
@@ -120,9 +125,10 @@ struct PairTables {
 };
 
 // Per-walker arrays in dynamic shared memory.  Walkers with one image and at
-// most kPairMatMax atoms also get a compact upper-triangle buffer holding one
-// float4 (force term) per unordered pair; the pair decode table is shared by
-// all walkers of a CTA (same atom count).
+// most kPairMatMax atoms also get the antisymmetric pair-force matrix, three
+// float planes [n][n|1] (the odd row stride keeps the row gather free of bank
+// conflicts); the pair decode table is shared by all walkers of a CTA (same
+// atom count).
 struct WalkArrays {
   float4* xs;           // [Nmax] position + type bits (current / trial positions)
   float* x0;            // [3 Nmax] saved positions
@@ -130,7 +136,7 @@ struct WalkArrays {
   float* dp;            // [3 Nmax] perturbed direction (flip target on reject)
   float* F;             // [3 Nmax] forces
   float* T;             // [2][3 n_img] image translations for cc[0], cc[1]
-  float4* pm;           // [Nmax(Nmax-1)/2] pair force terms, or nullptr
+  float* pm;            // [3][n][n|1] pair force terms g*dr_ij, or nullptr
   const uint16_t* pij;  // [Nmax(Nmax-1)/2] pair decode a | b << 8, or nullptr
 };
 
@@ -149,7 +155,7 @@ __host__ __device__ inline size_t walker_smem_bytes(int nmax, int nimg) {
   size_t b = align16(sizeof(WalkShared));
   b += 16u * (size_t)nmax + 4u * 12u * (size_t)nmax;
   b += align16(2u * 3u * 4u * (size_t)nimg);
-  if (use_pair_matrix(nmax, nimg)) b += 16u * pair_count(nmax);
+  if (use_pair_matrix(nmax, nimg)) b += align16(12u * (size_t)nmax * (size_t)(nmax | 1));
   return align16(b);
 }
 
@@ -169,7 +175,7 @@ __device__ inline WalkShared* carve_walker(char* p, int nmax, int nimg, const ui
   a.F = (float*)p; p += 12 * nmax;
   a.T = (float*)p; p += align16(2 * 3 * 4 * nimg);
   if (use_pair_matrix(nmax, nimg)) {
-    a.pm = (float4*)p;
+    a.pm = (float*)p;
     a.pij = pij;
   } else {
     a.pm = nullptr;
@@ -191,10 +197,6 @@ __device__ inline void build_pair_table(uint16_t* pij, int n) {
     const int b = p - a * (2 * n - a - 1) / 2 + a + 1;
     pij[p] = (uint16_t)(a | (b << 8));
   }
-}
-
-__device__ __forceinline__ int pair_index(int a, int b, int n) {
-  return a * (2 * n - a - 1) / 2 + (b - a - 1);
 }
 
 // Per-thread view of one walker and the group that walks it.  `par` is this
@@ -487,10 +489,10 @@ __device__ __forceinline__ void gather_tree(float& fx, float& fy, float& fz, int
   }
 }
 
-// Unordered pairs a < b once each (pair buffer path): the force term g*dr of
-// pair p goes to arr.pm[p]; atom i then gathers +pm[p(i,j)] for j > i and
-// -pm[p(j,i)] for j < i in float64 (the float32 term of the mirrored ordered
-// pair is exactly the negation).  U is the float64 sum over pairs.
+// Unordered pairs a < b once each (pair matrix path): the force term g*dr of
+// pair (a,b) goes to M[a][b] and its negation to M[b][a] (the float32 term of
+// the mirrored ordered pair is exactly the negation); atom i then gathers its
+// row in the canonical order.  U is the float64 sum over pairs.
 template <bool kForces, bool kS1, bool kDiag, class G>
 __device__ __forceinline__ void pairs_matrix(const JrParams& P, Walker<G>& w, const MicRegs& cc,
                                              double& U, double& sff, double& sfd) {
@@ -502,12 +504,11 @@ __device__ __forceinline__ void pairs_matrix(const JrParams& P, Walker<G>& w, co
   const float sig2_1 = w.tab.sig2[0], eps4_1 = w.tab.eps4[0], eps24_1 = w.tab.eps24[0];
   const int np = n * (n - 1) / 2;
   const int tid = w.g.rank(), gs = w.g.size();
+  const int S = n | 1, plane = n * S;
   double ep = 0.0;
-#pragma unroll 2
-  for (int p = tid; p < np; p += gs) {
-    const uint32_t ab = arr.pij[p];
-    const int a = ab & 255, b = ab >> 8;
-    const float4 xa = arr.xs[a], xb = arr.xs[b];
+  // Two pairs per trip with every shared-memory load issued before any store,
+  // so the pairs overlap (the compiler cannot move loads above the stores).
+  auto term = [&](const float4 xa, const float4 xb, float& e, float& vx, float& vy, float& vz) {
     float dx = __fsub_rn(xb.x, xa.x);
     float dy = __fsub_rn(xb.y, xa.y);
     float dz = __fsub_rn(xb.z, xa.z);
@@ -519,11 +520,37 @@ __device__ __forceinline__ void pairs_matrix(const JrParams& P, Walker<G>& w, co
       eps4 = w.tab.eps4[pt];
       eps24 = w.tab.eps24[pt];
     }
-    float e, g;
+    float g;
     lj_pair(dx, dy, dz, sig2, eps4, eps24, has_cut, rc2, e, g);
-    ep += (double)e;
-    if (kForces)
-      arr.pm[p] = make_float4(__fmul_rn(g, dx), __fmul_rn(g, dy), __fmul_rn(g, dz), 0.0f);
+    vx = __fmul_rn(g, dx);
+    vy = __fmul_rn(g, dy);
+    vz = __fmul_rn(g, dz);
+  };
+  auto put = [&](int a, int b, float vx, float vy, float vz) {
+    const int ab = a * S + b, ba = b * S + a;
+    arr.pm[ab] = vx;
+    arr.pm[ba] = -vx;
+    arr.pm[plane + ab] = vy;
+    arr.pm[plane + ba] = -vy;
+    arr.pm[2 * plane + ab] = vz;
+    arr.pm[2 * plane + ba] = -vz;
+  };
+  for (int p0 = tid; p0 < np; p0 += 2 * gs) {
+    const int p1 = p0 + gs;
+    const bool two = p1 < np;
+    const uint32_t ab0 = arr.pij[p0];
+    const uint32_t ab1 = two ? arr.pij[p1] : ab0;
+    const int a0 = ab0 & 255, b0 = ab0 >> 8, a1 = ab1 & 255, b1 = ab1 >> 8;
+    const float4 xa0 = arr.xs[a0], xb0 = arr.xs[b0], xa1 = arr.xs[a1], xb1 = arr.xs[b1];
+    float e0, vx0, vy0, vz0, e1, vx1, vy1, vz1;
+    term(xa0, xb0, e0, vx0, vy0, vz0);
+    term(xa1, xb1, e1, vx1, vy1, vz1);
+    ep += (double)e0;
+    if (two) ep += (double)e1;
+    if (kForces) {
+      put(a0, b0, vx0, vy0, vz0);
+      if (two) put(a1, b1, vx1, vy1, vz1);
+    }
   }
   if (!kForces) {
     double z0 = 0.0, z1 = 0.0;
@@ -540,32 +567,42 @@ __device__ __forceinline__ void pairs_matrix(const JrParams& P, Walker<G>& w, co
   double ff_part = 0.0, fd_part = 0.0;
   for (int base = 0; base < n; base += apb) {
     const int i = base + tid / L;
+    // warps whose atoms all lie beyond n leave the issue slots to the others
+    if (!__any_sync(0xffffffffu, i < n)) continue;
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
     // partners j0..j0+7 in ascending order; an absent partner adds +0, which
-    // leaves the running sum unchanged (it is never -0)
+    // leaves the running sum unchanged (it is never -0).  Absent partners read
+    // a clamped in-range element, so all 24 loads issue before the adds.
     const int j0 = blk * 8;
+    const int ic = i < n ? i : 0;
+    const float* row = arr.pm + ic * S;
+    float vx[8], vy[8], vz[8];
 #pragma unroll
     for (int jj = 0; jj < 8; ++jj) {
       const int j = j0 + jj;
       const bool ok = (i < n) && (j < n) && (j != i);
-      const bool up = i < j;
-      const int idx = ok ? (up ? pair_index(i, j, n) : pair_index(j, i, n)) : 0;
-      const float4 v = ok ? arr.pm[idx] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      const float vx = ok ? (up ? v.x : -v.x) : 0.0f;
-      const float vy = ok ? (up ? v.y : -v.y) : 0.0f;
-      const float vz = ok ? (up ? v.z : -v.z) : 0.0f;
-      fx = __fadd_rn(fx, vx);
-      fy = __fadd_rn(fy, vy);
-      fz = __fadd_rn(fz, vz);
+      const int jc = ok ? j : ic;
+      const float x = row[jc], y = row[plane + jc], z = row[2 * plane + jc];
+      vx[jj] = ok ? x : 0.0f;
+      vy[jj] = ok ? y : 0.0f;
+      vz[jj] = ok ? z : 0.0f;
+    }
+#pragma unroll
+    for (int jj = 0; jj < 8; ++jj) {
+      fx = __fadd_rn(fx, vx[jj]);
+      fy = __fadd_rn(fy, vy[jj]);
+      fz = __fadd_rn(fz, vz[jj]);
     }
     gather_tree(fx, fy, fz, L);
     if (blk == 0 && i < n) {
       arr.F[3 * i] = fx;
       arr.F[3 * i + 1] = fy;
       arr.F[3 * i + 2] = fz;
-      ff_part += (double)fx * (double)fx + (double)fy * (double)fy + (double)fz * (double)fz;
-      fd_part += (double)fx * (double)arr.dir[3 * i] + (double)fy * (double)arr.dir[3 * i + 1] +
-                 (double)fz * (double)arr.dir[3 * i + 2];
+      const double dx = fx, dy = fy, dz = fz;
+      ff_part = __fma_rn(dx, dx, __fma_rn(dy, dy, __fma_rn(dz, dz, ff_part)));
+      fd_part = __fma_rn(dx, (double)arr.dir[3 * i],
+                         __fma_rn(dy, (double)arr.dir[3 * i + 1],
+                                  __fma_rn(dz, (double)arr.dir[3 * i + 2], fd_part)));
     }
   }
   double e_part = ep;
