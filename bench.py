@@ -252,6 +252,10 @@ def run_ours(args):
     if rank != 0:
         return
     cpu = cpu_baseline(args) if (world == 1 and not args.no_cpu) else None
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "ns_iterate_kernel_lj32_8x512.json")
+    if os.path.exists(prof):
+        traffic = json.load(open(prof)).get("dram_bytes_per_launch")
     line = {
         "metric": METRIC, "value": value, "unit": "walker-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
@@ -266,7 +270,8 @@ def run_ours(args):
         "e2e": e2e,
         "gpu_launches": 2 * args.steps,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak > 0 else None, "traffic": None,
+                     "frac": achieved / peak if peak > 0 else None, "traffic": traffic,
+                     "traffic_unit": "DRAM bytes per ns_iterate_kernel launch (ncu capture)",
                      "peak_source": "measured FP32 FMA probe (jr_bench_fma_peak) on this GPU",
                      "peak_nominal": 148 * 128 * 2 * 1.965e-3,
                      "kernel": "ns_iterate_kernel", "flops_per_step": flops / args.steps},
