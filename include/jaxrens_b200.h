@@ -54,6 +54,7 @@ extern "C" {
 #define JR_MAX_IMAGES 125
 #define JR_MAX_CENTERS 8
 #define JR_MAX_ATOMS 256
+#define JR_MAX_CULL 32
 
 enum {
   JR_OK = 0,
@@ -62,7 +63,7 @@ enum {
   JR_ERR_CUDA = -3,        /* a CUDA runtime call failed */
   JR_ERR_TIMEOUT = -4,     /* a bounded device-side wait gave up */
   JR_ERR_WORKSPACE = -5,   /* workspace missing or too small */
-  JR_ERR_UNSUPPORTED = -6  /* feature outside this build (e.g. n_cull > 1) */
+  JR_ERR_UNSUPPORTED = -6  /* feature outside this build */
 };
 
 enum { JR_MODEL_LJ = 0, JR_MODEL_GAUSS_MIX = 1 };
@@ -76,7 +77,7 @@ typedef struct JrDims {
   int32_t n_moves;         /* M */
   int32_t n_mcmc_steps;    /* T */
   int32_t n_extra;         /* extra walked survivors per iteration */
-  int32_t n_cull;          /* culled walkers per iteration (this build: 1) */
+  int32_t n_cull;          /* culled walkers per iteration, 1..JR_MAX_CULL */
   int32_t shared_move_key; /* 1: move schedule from fold_in(rng_key[0], 1)
                               (VmapRuns); 0: from each run's own key */
 } JrDims;
@@ -114,7 +115,8 @@ typedef struct JrParams {
   JrModelParams model;
   JrMoveParams moves;
   double log_alpha;  /* log((K+1-n_cull)/(K+1)) */
-  double w_offset;   /* log dead weight offset of the iteration's cull */
+  double w_offset[JR_MAX_CULL];  /* log dead-weight offset of cull k of an iteration
+                                   (prior_mass.iteration_offsets) */
 } JrParams;
 
 typedef struct JrStateBuffers {
@@ -136,22 +138,25 @@ typedef struct JrStateBuffers {
   const float* mu;      /* NULL when the ensemble has no chemical potentials */
 } JrStateBuffers;
 
-/* Per-iteration outputs of jr_ns_iterate, leading axis n_iter then P.
+/* Per-iteration outputs of jr_ns_iterate, leading axis n_iter then P; the
+ * per-cull arrays carry an n_cull axis after P (absent in effect for
+ * n_cull = 1), culls in descending energy like the reference's worst_indices.
  * Any pointer may be NULL to skip that output. */
 typedef struct JrInfoBuffers {
-  int32_t* worst_idx;              /* [n_iter][P] */
-  int32_t* clone_idx;              /* [n_iter][P] */
-  double* emax;                    /* [n_iter][P] */
+  int32_t* worst_idx;              /* [n_iter][P][n_cull] */
+  int32_t* clone_idx;              /* [n_iter][P][n_cull] */
+  double* emax;                    /* [n_iter][P] the new contour (last cull) */
   double* log_evidence;            /* [n_iter][P] after the iteration */
-  float* dead_positions;           /* [n_iter][P][Nmax][3] */
-  int32_t* dead_types;             /* [n_iter][P][Nmax] */
-  float* dead_cell;                /* [n_iter][P][9] */
+  float* dead_positions;           /* [n_iter][P][n_cull][Nmax][3] */
+  int32_t* dead_types;             /* [n_iter][P][n_cull][Nmax] */
+  float* dead_cell;                /* [n_iter][P][n_cull][9] */
   int32_t* n_accepted;             /* [n_iter][P][M] */
   int32_t* n_proposed;             /* [n_iter][P][M] */
   int32_t* reject_reason_counts;   /* [n_iter][P][M][4] */
   int32_t* n_evaluations;          /* [n_iter][P][M] */
   int32_t* n_grad_evaluations;     /* [n_iter][P][M] */
   int32_t* rounds;                 /* [P] speculation rounds used (diagnostic) */
+  double* dead_energy;             /* [n_iter][P][n_cull] energies of the culled walkers */
 } JrInfoBuffers;
 
 /* Launch shape of the walk kernels.  threads: CTA size; tpa: threads per

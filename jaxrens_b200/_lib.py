@@ -11,6 +11,7 @@ import os
 
 MAX_SPECIES = 8
 MAX_MOVES = 8
+MAX_CULL = 32
 MAX_IMAGES = 125
 MAX_CENTERS = 8
 MAX_ATOMS = 256
@@ -80,7 +81,7 @@ class JrParams(C.Structure):
         ("model", JrModelParams),
         ("moves", JrMoveParams),
         ("log_alpha", C.c_double),
-        ("w_offset", C.c_double),
+        ("w_offset", C.c_double * MAX_CULL),
     ]
 
 
@@ -120,6 +121,7 @@ class JrInfoBuffers(C.Structure):
         ("n_evaluations", _vp),
         ("n_grad_evaluations", _vp),
         ("rounds", _vp),
+        ("dead_energy", _vp),
     ]
 
 

@@ -47,6 +47,9 @@ struct NsShared {
   int extras[kMaxWalk];
   int wset[kMaxWalk];
   int n_wset;
+  int cw[JR_MAX_CULL];     // n_cull > 1: culled walkers, descending energy
+  int cc[JR_MAX_CULL];     // n_cull > 1: their clone sources
+  double ce[JR_MAX_CULL];  // n_cull > 1: culled energies
   double res_E[kMaxWarps];  // final energy of each chain this CTA walked
   unsigned long long u64[2][kMaxWarps];
   int flag[2][kMaxWarps];
@@ -173,13 +176,15 @@ __device__ __forceinline__ void walk_chain(const JrParams& P, Walker<G>& w, int 
   w.g.sync();
 }
 
-// Copy the about-to-be-culled walker of replica p into info row `row`.
+// Copy the about-to-be-culled walker of replica p into info row `row`, cull
+// `cull` of that iteration.
 template <class G>
 __device__ inline void write_dead(const G& g, const JrDims& D, const JrStateBuffers& st,
-                                  const JrInfoBuffers& info, int row, int p, int slot, int n) {
+                                  const JrInfoBuffers& info, int row, int p, int slot, int n,
+                                  int cull) {
   const int K = D.n_walkers, Nmax = D.n_atoms_max, Pn = D.n_replicas;
   const size_t wb = (size_t)p * K + slot;
-  const size_t ib = (size_t)row * Pn + p;
+  const size_t ib = ((size_t)row * Pn + p) * D.n_cull + cull;
   const int r0 = g.rank(), gs = g.size();
   if (info.dead_positions)
     for (int q = r0; q < 3 * n; q += gs)
@@ -198,31 +203,109 @@ __device__ inline void copy_params(JrParams& dst, const JrParams& src) {
   for (int q = threadIdx.x; q < nw; q += blockDim.x) d[q] = s[q];
 }
 
-// Dynamic smem of the NS kernel: [K doubles][K floats][pair table][walkers].
+// Dynamic smem of the NS kernel: [K doubles][K floats](n_cull > 1: 3 x
+// [K ints])[pair table][walkers].
 struct DynLayout {
   double* Epop;
   float* noise;
+  int* order;     // n_cull > 1: walkers by descending energy, then survivors
+  int* tmp;       // n_cull > 1: shuffle scratch
+  uint32_t* u;    // n_cull > 1: shuffle sort keys
   uint16_t* pij;
   char* walkers;
   size_t walker_bytes;
 };
 
-__host__ __device__ inline size_t dyn_head_bytes(int K, int nmax, int nimg) {
-  return align16(8u * (size_t)K) + align16(4u * (size_t)K) + pair_table_bytes(nmax, nimg);
+__host__ __device__ inline size_t dyn_head_bytes(int K, int nmax, int nimg, int ncull) {
+  return align16(8u * (size_t)K) + align16(4u * (size_t)K) +
+         (ncull > 1 ? 3u * align16(4u * (size_t)K) : 0u) + pair_table_bytes(nmax, nimg);
 }
 
-__device__ inline DynLayout dyn_layout(unsigned char* dyn, int K, int nmax, int nimg) {
+__device__ inline DynLayout dyn_layout(unsigned char* dyn, int K, int nmax, int nimg, int ncull) {
   DynLayout L;
   char* p = reinterpret_cast<char*>(dyn);
   L.Epop = reinterpret_cast<double*>(p);
   p += align16(8u * (size_t)K);
   L.noise = reinterpret_cast<float*>(p);
   p += align16(4u * (size_t)K);
+  L.order = L.tmp = nullptr;
+  L.u = nullptr;
+  if (ncull > 1) {
+    L.order = reinterpret_cast<int*>(p);
+    p += align16(4u * (size_t)K);
+    L.tmp = reinterpret_cast<int*>(p);
+    p += align16(4u * (size_t)K);
+    L.u = reinterpret_cast<uint32_t*>(p);
+    p += align16(4u * (size_t)K);
+  }
   L.pij = use_pair_matrix(nmax, nimg) ? reinterpret_cast<uint16_t*>(p) : nullptr;
   p += pair_table_bytes(nmax, nimg);
   L.walkers = p;
   L.walker_bytes = walker_smem_bytes(nmax, nimg);
   return L;
+}
+
+// _select_culls for n_cull > 1 (nested_sampling.py:195-212).  order = the
+// walkers by descending energy (NaN last, as XLA's float sort places it),
+// then descending uniform noise, then index (lexsort((-noise, -E)));
+// worst = order[:n_cull].  The survivors order[n_cull:] are shuffled like
+// jax.random.permutation on an array: ceil(3 ln n / ln(2^32 - 1)) rounds
+// (1 for n <= 1625, 2 up to 2642245), each splitting the key and stably
+// sorting by 32-bit random bits; clone = survivors[:n_cull], extras =
+// survivors[n_cull:n_cull + n_extra].  CTA-wide, ranks by counting.
+__device__ void select_culls_multi(NsShared& ns, const DynLayout& L, const double* E, int K,
+                                   int ncull, int nx, Key kworst, Key kclone) {
+  for (int k = threadIdx.x; k < K; k += blockDim.x) L.noise[k] = uniform01(bits32(kworst, (uint32_t)k));
+  __syncthreads();
+  for (int k = threadIdx.x; k < K; k += blockDim.x) {
+    const double ek = E[k];
+    const bool nk = isnan(ek);
+    const float zk = L.noise[k];
+    int r = 0;
+    for (int j = 0; j < K; ++j) {
+      const double ej = E[j];
+      const bool nj = isnan(ej);
+      bool before;
+      if (nj != nk) before = nk;
+      else if (!nj && ej != ek) before = ej > ek;
+      else if (L.noise[j] != zk) before = L.noise[j] > zk;
+      else before = j < k;
+      r += before ? 1 : 0;
+    }
+    L.order[r] = k;
+  }
+  __syncthreads();
+  const int n = K - ncull;
+  int* x = L.order + ncull;
+  const int rounds = n <= 1 ? 0 : (n <= 1625 ? 1 : 2);
+  Key key = kclone;
+  for (int rd = 0; rd < rounds; ++rd) {
+    const Key sub = split(key, 1u);
+    key = split(key, 0u);
+    for (int m = threadIdx.x; m < n; m += blockDim.x) L.u[m] = bits32(sub, (uint32_t)m);
+    __syncthreads();
+    for (int m = threadIdx.x; m < n; m += blockDim.x) {
+      const uint32_t um = L.u[m];
+      int pos = 0;
+      for (int q = 0; q < n; ++q) {
+        const uint32_t uq = L.u[q];
+        pos += (uq < um || (uq == um && q < m)) ? 1 : 0;
+      }
+      L.tmp[pos] = x[m];
+    }
+    __syncthreads();
+    for (int m = threadIdx.x; m < n; m += blockDim.x) x[m] = L.tmp[m];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    for (int c = 0; c < ncull; ++c) {
+      ns.cw[c] = L.order[c];
+      ns.cc[c] = x[c];
+      ns.ce[c] = E[L.order[c]];
+    }
+    for (int e = 0; e < nx; ++e) ns.extras[e] = x[ncull + e];
+  }
+  __syncthreads();
 }
 
 template <class G>
@@ -265,15 +348,16 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
   const int p = blockIdx.x / C;
   const int c = blockIdx.x % C;
   const int K = D.n_walkers, M = D.n_moves, T = D.n_mcmc_steps;
-  const int nx = D.n_extra, W = 1 + nx;
+  const int nx = D.n_extra, ncull = D.n_cull, W = ncull + nx;
   const int n = min(max(st.n_atoms[p], 1), D.n_atoms_max);
   const int nimg = Pg.model.n_images;
   const int cpc = kWarp ? (int)(blockDim.x >> 5) : 1;  // chains per CTA
   const int my = kWarp ? (int)(threadIdx.x >> 5) : 0;  // this group's chain in the CTA
   const int slots = C * cpc;
   const int s_my = c * cpc + my;
-  const int Dmax = (slots >= 2 * W) ? (slots / W < kMaxD ? slots / W : kMaxD) : 1;
-  DynLayout L = dyn_layout(dyn, K, D.n_atoms_max, nimg);
+  // speculation needs the n_cull = 1 selection (the top of the order only)
+  const int Dmax = (ncull == 1 && slots >= 2 * W) ? (slots / W < kMaxD ? slots / W : kMaxD) : 1;
+  DynLayout L = dyn_layout(dyn, K, D.n_atoms_max, nimg, D.n_cull);
   WalkArrays arr;
   WalkShared* wsp = carve_walker(L.walkers + (size_t)my * L.walker_bytes, D.n_atoms_max, nimg,
                                  L.pij, arr);
@@ -301,6 +385,21 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
       const Key ka = split(kd, 0u), kw = split(kd, 1u);
       const Key kclone = split(ka, 1u), kextra = split(ka, 2u);
       const Key kmcmc = split(ka, 3u), kmoves = split(ka, 4u);
+      if (ncull > 1) {  // Dr == 1 here
+        select_culls_multi(ns, L, L.Epop, K, ncull, nx, kw, kclone);
+        if (threadIdx.x == 0) {
+          ns.spec[0] = 1;
+          ns.worst[0] = ns.cw[0];
+          ns.clone[0] = ns.cc[0];
+          ns.e[0] = ns.ce[ncull - 1];
+          ns.kmcmc[0] = kmcmc;
+          ns.kmove[0] = D.shared_move_key ? split(k0d, 1u) : kmoves;
+        }
+        __syncthreads();
+        kd = split(ka, 0u);
+        k0d = advance_iteration(k0d);
+        continue;
+      }
       int worst;
       double emax;
       bool any_nan;
@@ -338,10 +437,11 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
     __syncthreads();
     if (Dmax == 1) {
       for (int sidx = s_my; sidx < W; sidx += slots) {
-        const int src = sidx == 0 ? ns.clone[0] : ns.extras[sidx - 1];
-        const int dst = sidx == 0 ? ns.worst[0] : src;
-        if (sidx == 0) write_dead(w.g, D, st, info, committed, p, ns.worst[0], n);
-        load_walker(P, D, st, w, p, src, sidx == 0);
+        const bool is_clone = sidx < ncull;
+        const int src = is_clone ? (ncull > 1 ? ns.cc[sidx] : ns.clone[0]) : ns.extras[sidx - ncull];
+        const int dst = is_clone ? (ncull > 1 ? ns.cw[sidx] : ns.worst[0]) : src;
+        if (is_clone) write_dead(w.g, D, st, info, committed, p, dst, n, sidx);
+        load_walker(P, D, st, w, p, src, is_clone);
         walk_chain(P, w, T, split(ns.kmcmc[0], (uint32_t)sidx), ns.kmove[0], ns.e[0], pressure,
                    mu);
         store_walker(D, st, w, p, dst);
@@ -376,7 +476,7 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
       const int d = s_my / W, wi = s_my % W;
       if (d < nval) {
         const int dst = wi == 0 ? ns.worst[d] : ns.extras[d * nx + wi - 1];
-        if (wi == 0) write_dead(w.g, D, st, info, committed + d, p, ns.worst[d], n);
+        if (wi == 0) write_dead(w.g, D, st, info, committed + d, p, ns.worst[d], n, 0);
         store_walker(D, st, w, p, dst);
       }
     }
@@ -406,10 +506,30 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
           if (info.reject_reason_counts)
             for (int q = 0; q < 4; ++q) info.reject_reason_counts[(ib * M + m) * 4 + q] = rr[q];
         }
-        const double lw = (double)it * P.log_alpha + P.w_offset;
-        logZ = logaddexp(logZ, lw - ns.e[d]);
-        if (info.worst_idx) info.worst_idx[ib] = ns.worst[d];
-        if (info.clone_idx) info.clone_idx[ib] = ns.clone[d];
+        if (ncull == 1) {
+          const double lw = (double)it * P.log_alpha + P.w_offset[0];
+          logZ = logaddexp(logZ, lw - ns.e[d]);
+          if (info.worst_idx) info.worst_idx[ib] = ns.worst[d];
+          if (info.clone_idx) info.clone_idx[ib] = ns.clone[d];
+          if (info.dead_energy) info.dead_energy[ib] = ns.e[d];
+        } else {
+          // logsumexp over the culls (jax.nn.logsumexp with its finite shift)
+          double lw[JR_MAX_CULL];
+          double amax = -INFINITY;
+          for (int q = 0; q < ncull; ++q) {
+            lw[q] = (double)it * P.log_alpha + P.w_offset[q] - ns.ce[q];
+            if (lw[q] > amax || isnan(lw[q])) amax = lw[q];
+          }
+          if (!isfinite(amax)) amax = 0.0;
+          double sum = 0.0;
+          for (int q = 0; q < ncull; ++q) sum += exp(lw[q] - amax);
+          logZ = logaddexp(logZ, log(sum) + amax);
+          for (int q = 0; q < ncull; ++q) {
+            if (info.worst_idx) info.worst_idx[ib * ncull + q] = ns.cw[q];
+            if (info.clone_idx) info.clone_idx[ib * ncull + q] = ns.cc[q];
+            if (info.dead_energy) info.dead_energy[ib * ncull + q] = ns.ce[q];
+          }
+        }
         if (info.emax) info.emax[ib] = ns.e[d];
         if (info.log_evidence) info.log_evidence[ib] = logZ;
       }
@@ -733,6 +853,7 @@ JrLaunchConfig heuristic_config(const JrDims* d) {
 
 // Speculation depth bound of check_config, without setting the error text.
 bool spec_fits(const JrLaunchConfig& c, const JrDims* d) {
+  if (d->n_cull > 1) return true;  // n_cull > 1 never speculates
   const int W = 1 + d->n_extra;
   const int slots = c.cluster * (c.warp_walkers ? c.threads / 32 : 1);
   if (slots < 2 * W) return true;
@@ -761,9 +882,11 @@ JrLaunchConfig ns_heuristic_config(const JrDims* d, int n_iter) {
     cudaGetLastError();
     sms = 148;
   }
-  const int W = 1 + d->n_extra;
+  const int W = d->n_cull + d->n_extra;
   const int cpc = c.warp_walkers ? c.threads / 32 : 1;
-  const int want = (n_iter > 0 ? n_iter : 1) * W;              // chains one launch can use
+  // chains one launch can run at once: n_iter * W speculated (n_cull = 1),
+  // otherwise the W chains of one iteration
+  const int want = d->n_cull > 1 ? W : (n_iter > 0 ? n_iter : 1) * W;
   int cl = (want + cpc - 1) / cpc;
   const int fit = (sms * 11 / 20) / (d->n_replicas > 0 ? d->n_replicas : 1);
   if (cl > 10) cl = 10;
@@ -782,9 +905,14 @@ int check_params(const JrDims* d, const JrParams* p) {
                                   std::to_string(JR_MAX_ATOMS));
   if (d->n_moves < 1 || d->n_moves > JR_MAX_MOVES || d->n_moves != p->moves.n_moves)
     return fail(JR_ERR_SHAPE, "n_moves must be in [1, 8] and match params.moves");
-  if (d->n_cull != 1) return fail(JR_ERR_UNSUPPORTED, "this build implements n_cull == 1 only");
-  if (d->n_extra < 0 || d->n_extra > d->n_walkers - 2 || d->n_extra + 1 > jr::kMaxWalk)
-    return fail(JR_ERR_SHAPE, "n_extra must satisfy 0 <= n_extra <= n_walkers-2 and <= 255");
+  if (d->n_cull < 1 || d->n_cull > JR_MAX_CULL)
+    return fail(JR_ERR_SHAPE, "n_cull must be in [1, " + std::to_string(JR_MAX_CULL) + "]");
+  if (d->n_extra < 0 || d->n_extra > d->n_walkers - 2 || d->n_extra + d->n_cull > jr::kMaxWalk)
+    return fail(JR_ERR_SHAPE, "n_extra must satisfy 0 <= n_extra <= n_walkers-2 and "
+                              "n_cull + n_extra <= 256");
+  if (d->n_cull > 1 && 2 * d->n_cull + d->n_extra > d->n_walkers)
+    return fail(JR_ERR_SHAPE, "n_cull > 1 needs 2*n_cull + n_extra <= n_walkers "
+                              "(nested_sampling.py _select_culls)");
   if (p->model.n_species < 1 || p->model.n_species > JR_MAX_SPECIES)
     return fail(JR_ERR_PARAM, "n_species must be in [1, 8]");
   if (p->model.n_images < 1 || p->model.n_images > JR_MAX_IMAGES)
@@ -813,7 +941,7 @@ int check_config(const JrLaunchConfig& c, const JrDims* d) {
     return fail(JR_ERR_PARAM, "warp-walker CTAs hold at most 4 walkers (128 threads)");
   const int W = 1 + d->n_extra;
   const int slots = c.cluster * (c.warp_walkers ? c.threads / 32 : 1);
-  if (slots >= 2 * W) {
+  if (d->n_cull == 1 && slots >= 2 * W) {
     const int D = slots / W < jr::kMaxD ? slots / W : jr::kMaxD;
     if (D * d->n_extra > jr::kMaxWalk || D * W > jr::kMaxWalk)
       return fail(JR_ERR_PARAM, "speculation depth * n_extra too large");
@@ -823,7 +951,7 @@ int check_config(const JrLaunchConfig& c, const JrDims* d) {
 
 size_t ns_dyn_smem(const JrDims* d, const JrParams* p, const JrLaunchConfig& c) {
   const int cpc = c.warp_walkers ? c.threads / 32 : 1;
-  return jr::dyn_head_bytes(d->n_walkers, d->n_atoms_max, p->model.n_images) +
+  return jr::dyn_head_bytes(d->n_walkers, d->n_atoms_max, p->model.n_images, d->n_cull) +
          (size_t)cpc * jr::walker_smem_bytes(d->n_atoms_max, p->model.n_images);
 }
 

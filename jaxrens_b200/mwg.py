@@ -36,11 +36,19 @@ class MWGStep:
     def move_names(self) -> list[str]:
         return [d.name for d in self.move_descriptors]
 
-    def with_evidence(self, log_alpha: float, w_offset: float) -> _lib.JrParams:
+    def with_evidence(self, log_alpha: float, w_offset) -> _lib.JrParams:
+        """Parameters with the prior-mass constants of one iteration:
+        ``log_alpha`` and the dead-weight offsets ``w_offset`` (a scalar for
+        n_cull = 1 or the ``(n_cull,)`` array of
+        ``prior_mass.iteration_offsets``)."""
         p = _lib.JrParams()
         C.pointer(p)[0] = self.params
         p.log_alpha = log_alpha
-        p.w_offset = w_offset
+        wo = np.atleast_1d(np.asarray(w_offset, np.float64))
+        if wo.size > _lib.MAX_CULL:
+            raise ValueError(f"at most {_lib.MAX_CULL} culls per iteration")
+        for k, v in enumerate(wo):
+            p.w_offset[k] = float(v)
         return p
 
 

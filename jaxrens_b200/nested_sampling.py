@@ -263,20 +263,23 @@ def _apply_restart(ns: NSState, rs) -> None:
 class InfoBuffers:
     """Device buffers for ``n_iter`` iterations of per-iteration outputs."""
 
-    def __init__(self, ns: NSState, M: int, n_iter: int, dead: bool = True):
+    def __init__(self, ns: NSState, M: int, n_iter: int, dead: bool = True, n_cull: int = 1):
         import torch
 
         dev = ns.population.positions.device
         P, K, Nmax = ns.population.types.shape
         z = lambda shape, dt: torch.zeros(shape, dtype=dt, device=dev)
+        c = () if n_cull == 1 else (n_cull,)   # per-cull axis after P when n_cull > 1
         self.n_iter = n_iter
-        self.worst_idx = z((n_iter, P), torch.int32)
-        self.clone_idx = z((n_iter, P), torch.int32)
+        self.n_cull = n_cull
+        self.worst_idx = z((n_iter, P) + c, torch.int32)
+        self.clone_idx = z((n_iter, P) + c, torch.int32)
+        self.dead_energy = z((n_iter, P) + c, torch.float64)
         self.emax = z((n_iter, P), torch.float64)
         self.log_evidence = z((n_iter, P), torch.float64)
-        self.dead_positions = z((n_iter, P, Nmax, 3), torch.float32) if dead else None
-        self.dead_types = z((n_iter, P, Nmax), torch.int32) if dead else None
-        self.dead_cell = z((n_iter, P, 3, 3), torch.float32) if dead else None
+        self.dead_positions = z((n_iter, P) + c + (Nmax, 3), torch.float32) if dead else None
+        self.dead_types = z((n_iter, P) + c + (Nmax,), torch.int32) if dead else None
+        self.dead_cell = z((n_iter, P) + c + (3, 3), torch.float32) if dead else None
         self.n_accepted = z((n_iter, P, M), torch.int32)
         self.n_proposed = z((n_iter, P, M), torch.int32)
         self.reject_reason_counts = z((n_iter, P, M, 4), torch.int32)
@@ -295,15 +298,15 @@ def ns_iterate(ns_state: NSState, step_fn: MWGStep, n_iter: int, n_mcmc_steps: i
                n_extra: int = 0, n_cull: int = 1, info: InfoBuffers | None = None,
                cfg: _lib.JrLaunchConfig | None = None) -> InfoBuffers:
     """Run ``n_iter`` NS iterations on every run in one launch."""
-    if n_cull != 1:
-        raise NotImplementedError("this build implements n_cull == 1 (the reference default)")
     K = ns_state.n_walkers
     la = prior_mass.log_alpha(K, n_cull)
     _, w_off = prior_mass.iteration_offsets(K, n_cull)
-    params = step_fn.with_evidence(la, float(w_off[0]))
+    params = step_fn.with_evidence(la, w_off)
     dims = make_dims(ns_state, step_fn, n_mcmc_steps, n_extra, n_cull)
     if info is None:
-        info = InfoBuffers(ns_state, step_fn.n_moves, n_iter)
+        info = InfoBuffers(ns_state, step_fn.n_moves, n_iter, n_cull=n_cull)
+    if info.n_cull != n_cull:
+        raise ValueError("info buffers were sized for a different n_cull")
     sb = state_buffers(ns_state)
     ib = info.cstruct()
     rc = _lib.load().jr_ns_iterate(
@@ -317,31 +320,39 @@ def ns_iterate(ns_state: NSState, step_fn: MWGStep, n_iter: int, n_mcmc_steps: i
 def info_dict(info: InfoBuffers, ns_state: NSState, n_mcmc_steps: int, n_extra: int,
               row: int = 0) -> dict:
     """The reference's ``info`` dict (``nested_sampling.py:653-685``) for one
-    iteration, leading run axis ``(P, ...)``; device tensors."""
+    iteration, leading run axis ``(P, ...)``; device tensors.  The
+    single-walker views (``worst_idx``, ``dead_walker``) are the contour cull,
+    the last of the ``(n_cull,)``-wide ones."""
     import torch
 
     emax64 = info.emax[row]
-    pop = ns_state.population
-    dead_energy = emax64
-    dw = {
-        "positions": None if info.dead_positions is None else info.dead_positions[row],
-        "types": None if info.dead_types is None else info.dead_types[row],
-        "energy": dead_energy.to(torch.float32),
-        "cell": None if info.dead_cell is None else info.dead_cell[row],
+    multi = info.n_cull > 1
+
+    def wide(t):   # (P, n_cull, ...) view
+        return None if t is None else (t[row] if multi else t[row][:, None])
+
+    dws = {
+        "positions": wide(info.dead_positions),
+        "types": wide(info.dead_types),
+        "energy": wide(info.dead_energy).to(torch.float32),
+        "cell": wide(info.dead_cell),
     }
+    dw = {k: (None if v is None else v[:, -1]) for k, v in dws.items()}
     n_acc = info.n_accepted[row]
-    total = (n_mcmc_steps * (1 + n_extra))
+    total = n_mcmc_steps * (info.n_cull + n_extra)
+    worst = wide(info.worst_idx)
+    clone = wide(info.clone_idx)
     d = {
         "emax": emax64.to(torch.float32),
         "emax64": emax64,
         "hmax": emax64.to(torch.float32),
-        "worst_idx": info.worst_idx[row],
-        "clone_idx": info.clone_idx[row],
-        "worst_indices": info.worst_idx[row][:, None],
-        "clone_indices": info.clone_idx[row][:, None],
+        "worst_idx": worst[:, -1],
+        "clone_idx": clone[:, -1],
+        "worst_indices": worst,
+        "clone_indices": clone,
         "acceptance_rate": n_acc.sum(-1).to(torch.float32) / float(total),
         "dead_walker": dw,
-        "dead_walkers": {k: (None if v is None else v[:, None]) for k, v in dw.items()},
+        "dead_walkers": dws,
         "n_accepted_per_move": n_acc,
         "n_proposed_per_move": info.n_proposed[row],
         "reject_reason_counts_per_move": info.reject_reason_counts[row],
@@ -349,7 +360,6 @@ def info_dict(info: InfoBuffers, ns_state: NSState, n_mcmc_steps: int, n_extra: 
         "n_grad_evaluations_per_move": info.n_grad_evaluations[row],
         "log_evidence": info.log_evidence[row],
     }
-    del pop
     return d
 
 
@@ -364,13 +374,13 @@ def ns_step(ns_state: NSState, step_fn: MWGStep, n_mcmc_steps: int = 20, n_extra
     return ns_state, info_dict(info, ns_state, n_mcmc_steps, n_extra, 0)
 
 
-def final_log_evidence(ns_state: NSState):
+def final_log_evidence(ns_state: NSState, n_cull: int = 1):
     """Live-walker share of the remaining prior mass added to log Z
     (``nested_sampling.py:229-252``), float64, per run."""
     import torch
 
     K = ns_state.n_walkers
-    la = prior_mass.log_alpha(K, 1)
+    la = prior_mass.log_alpha(K, n_cull)
     log_x = ns_state.iteration.to(torch.float64) * la + (math.log(K) - math.log(K + 1.0))
     log_live = log_x - math.log(K) + torch.logsumexp(-ns_state.population.energy64, dim=-1)
     return torch.logaddexp(ns_state.log_evidence, log_live)
@@ -544,16 +554,17 @@ def run_loop(ns_state: NSState, step_fn: MWGStep, n_mcmc_steps: int, n_extra: in
 def run_ns(positions, types, energies, cells, init_fn, step_fn, rng_key,
            max_iterations: int = 1000, n_mcmc_steps: int = 20, n_extra: int = 0,
            convergence_threshold: float | None = None, callbacks=None,
-           ensemble_params=None, step_sizes=None, check_interval: int = 1):
+           ensemble_params=None, step_sizes=None, check_interval: int = 1,
+           n_cull: int = 1):
     """Single run to termination (``nested_sampling.py:1065-1226``)."""
     ns = init_ns(init_fn, positions, types, energies, cells, rng_key,
                  step_sizes=step_sizes, ensemble_params=ensemble_params)
     crit = [IterationTermination(max_iterations)]
     if convergence_threshold is not None:
-        crit.append(PriorMassTermination(ns.n_walkers, convergence_threshold))
-    run_loop(ns, step_fn, n_mcmc_steps, n_extra, crit, callbacks,
+        crit.append(PriorMassTermination(ns.n_walkers, convergence_threshold, n_cull))
+    run_loop(ns, step_fn, n_mcmc_steps, n_extra, crit, callbacks, n_cull=n_cull,
              check_interval=check_interval)
-    return {"ns_state": ns, "log_evidence": final_log_evidence(ns),
+    return {"ns_state": ns, "log_evidence": final_log_evidence(ns, n_cull),
             "n_iterations": ns.iteration}
 
 
@@ -561,19 +572,20 @@ def run_ns_parallel(positions, types, energies, cells, init_fn, step_fn, rng_key
                     max_iterations: int = 1000, n_mcmc_steps: int = 20, n_extra: int = 0,
                     convergence_threshold: float | None = None, callbacks=None,
                     ensemble_params=None, re_interval: int = 0, n_swap_cycles: int = 1,
-                    re_key=None, step_sizes=None, check_interval: int = 1):
+                    re_key=None, step_sizes=None, check_interval: int = 1,
+                    n_cull: int = 1):
     """R runs batched (``nested_sampling.py:1341-1560``), with optional
     replica exchange every ``re_interval`` iterations."""
     ns = init_ns_parallel(init_fn, positions, types, energies, cells, rng_keys,
                           step_sizes=step_sizes, ensemble_params=ensemble_params)
     crit = [IterationTermination(max_iterations)]
     if convergence_threshold is not None:
-        crit.append(PriorMassTermination(ns.n_walkers, convergence_threshold))
+        crit.append(PriorMassTermination(ns.n_walkers, convergence_threshold, n_cull))
     re = None
     if re_interval > 0 and ns.n_runs > 1:
         re = InterREManager(re_interval, n_swap_cycles,
                             re_key if re_key is not None else prng.key(0))
     run_loop(ns, step_fn, n_mcmc_steps, n_extra, crit, callbacks, inter_re=re,
-             check_interval=check_interval)
-    return {"ns_state": ns, "log_evidence": final_log_evidence(ns),
+             n_cull=n_cull, check_interval=check_interval)
+    return {"ns_state": ns, "log_evidence": final_log_evidence(ns, n_cull),
             "n_iterations": ns.iteration}

@@ -910,7 +910,7 @@ int32_t jro_mwg_step(const JroModel* mdl, const JroMoves* mv, int32_t mode,
 }
 
 /* ------------------------------------------------------------------ */
-/* ns_step (sampling/nested_sampling.py:391-686), n_cull = 1            */
+/* ns_step (sampling/nested_sampling.py:391-686)                        */
 /* ------------------------------------------------------------------ */
 
 static double logaddexp(double a, double b) {
@@ -930,11 +930,60 @@ static void copy_walker(JroReplica* r, int dst, int src, int M) {
   r->energy[dst] = r->energy[src];
 }
 
-void jro_ns_step(const JroModel* mdl, const JroMoves* mv, int32_t mode,
-                 JroReplica* rep, int32_t T, int32_t n_extra,
-                 const uint32_t* move_key_in, double log_alpha, double w_offset,
-                 JroIterInfo* info, float* dead_x, int32_t* dead_t,
-                 float* dead_c) {
+/* jax.random.permutation of an array (jax/_src/random.py _shuffle, a
+ * published algorithm): num_rounds = ceil(3 ln(max(1,n)) / ln(2^32 - 1))
+ * rounds, each splitting the key (key, subkey = split(key)) and stably
+ * sorting the array by 32-bit random_bits(subkey, 32, (n,)). */
+static void jax_shuffle(const uint32_t key_in[2], int32_t* x, int n) {
+  uint32_t key[2] = {key_in[0], key_in[1]};
+  const int rounds = (int)ceil(3.0 * log((double)(n > 1 ? n : 1)) / log(4294967295.0));
+  uint32_t* u = (uint32_t*)malloc(sizeof(uint32_t) * (n > 0 ? n : 1));
+  int32_t* y = (int32_t*)malloc(sizeof(int32_t) * (n > 0 ? n : 1));
+  for (int r = 0; r < rounds; ++r) {
+    uint32_t nk[2], sub[2];
+    jro_split(key, 0, nk);
+    jro_split(key, 1, sub);
+    key[0] = nk[0];
+    key[1] = nk[1];
+    for (int m = 0; m < n; ++m) u[m] = jro_bits32(sub, (uint32_t)m);
+    for (int m = 0; m < n; ++m) {  /* stable: rank by (u, position) */
+      int pos = 0;
+      for (int q = 0; q < n; ++q)
+        if (u[q] < u[m] || (u[q] == u[m] && q < m)) ++pos;
+      y[pos] = x[m];
+    }
+    memcpy(x, y, sizeof(int32_t) * n);
+  }
+  free(u);
+  free(y);
+}
+
+/* lexsort((-noise, -E)) order key: energies descending (NaN last, as in
+ * XLA's float sort), then noise descending, then index ascending. */
+static int cull_before(const double* E, const float* nz, int j, int k) {
+  const int nj = isnan(E[j]), nk = isnan(E[k]);
+  if (nj != nk) return nk;
+  if (!nj && E[j] != E[k]) return E[j] > E[k];
+  if (nz[j] != nz[k]) return nz[j] > nz[k];
+  return j < k;
+}
+
+static double logsumexp_d(const double* v, int n) {
+  double amax = -INFINITY;
+  for (int i = 0; i < n; ++i)
+    if (v[i] > amax || isnan(v[i])) amax = v[i];
+  if (!isfinite(amax)) amax = 0.0;
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) s += exp(v[i] - amax);
+  return log(s) + amax;
+}
+
+void jro_ns_step_n(const JroModel* mdl, const JroMoves* mv, int32_t mode,
+                   JroReplica* rep, int32_t T, int32_t n_cull, int32_t n_extra,
+                   const uint32_t* move_key_in, double log_alpha,
+                   const double* w_offsets, JroIterInfo* info, int32_t* worst_out,
+                   int32_t* clone_out, double* dead_E_out, float* dead_x,
+                   int32_t* dead_t, float* dead_c) {
   const int K = rep->n_walkers, N = rep->n_atoms, M = mv->n_moves;
   uint32_t key[2] = {rep->rng_key[0], rep->rng_key[1]};
   uint32_t k_a[2], k_worst[2], k_next[2], k_clone[2], k_extra[2], k_mcmc[2], k_moves[2];
@@ -948,65 +997,107 @@ void jro_ns_step(const JroModel* mdl, const JroMoves* mv, int32_t mode,
   uint32_t move_key[2];
   if (move_key_in) { move_key[0] = move_key_in[0]; move_key[1] = move_key_in[1]; }
   else { move_key[0] = k_moves[0]; move_key[1] = k_moves[1]; }
-
-  /* _find_worst_walker (nested_sampling.py:86-109): jnp.max propagates NaN */
-  double emax = rep->energy[0];
-  int any_nan = 0;
-  for (int k = 0; k < K; ++k) {
-    if (isnan(rep->energy[k])) any_nan = 1;
-    if (rep->energy[k] > emax) emax = rep->energy[k];
-  }
-  if (any_nan) emax = NAN;
-  int worst = 0;
-  float best = -INFINITY;
-  int found = 0;
-  for (int k = 0; k < K; ++k) {
-    if (rep->energy[k] == emax) {
-      float nz = jro_uniform(jro_bits32(k_worst, (uint32_t)k), 0.0f, 1.0f);
-      if (!found || nz > best) { best = nz; worst = k; found = 1; }
-    }
-  }
-  /* clone (nested_sampling.py:182-183) */
-  int clone = jro_randint(k_clone, 0, K - 1);
-  if (clone >= worst) clone += 1;
-  /* extras (nested_sampling.py:112-133): stable argsort of -noise */
-  int W = 1 + n_extra;
+  const int W = n_cull + n_extra;
+  int* worst = (int*)malloc(sizeof(int) * n_cull);
+  int* clone = (int*)malloc(sizeof(int) * n_cull);
   int* walk = (int*)malloc(sizeof(int) * W);
-  walk[0] = worst;
-  if (n_extra > 0) {
-    float* nz = (float*)malloc(sizeof(float) * K);
-    for (int k = 0; k < K; ++k) nz[k] = jro_uniform(jro_bits32(k_extra, (uint32_t)k), 0.0f, 1.0f);
-    nz[worst] = -INFINITY;
-    nz[clone] = -INFINITY;
-    char* used = (char*)calloc(K, 1);
-    for (int e = 0; e < n_extra; ++e) {
-      int bi = -1;
-      for (int k = 0; k < K; ++k)
-        if (!used[k] && (bi < 0 || nz[k] > nz[bi])) bi = k;
-      used[bi] = 1;
-      walk[1 + e] = bi;
+  double emax;
+  if (n_cull == 1) {
+    /* _find_worst_walker (nested_sampling.py:86-109): jnp.max propagates NaN */
+    emax = rep->energy[0];
+    int any_nan = 0;
+    for (int k = 0; k < K; ++k) {
+      if (isnan(rep->energy[k])) any_nan = 1;
+      if (rep->energy[k] > emax) emax = rep->energy[k];
     }
-    free(used);
+    if (any_nan) emax = NAN;
+    int w0 = 0;
+    float best = -INFINITY;
+    int found = 0;
+    for (int k = 0; k < K; ++k) {
+      if (rep->energy[k] == emax) {
+        float nz = jro_uniform(jro_bits32(k_worst, (uint32_t)k), 0.0f, 1.0f);
+        if (!found || nz > best) { best = nz; w0 = k; found = 1; }
+      }
+    }
+    /* clone (nested_sampling.py:182-183) */
+    int c0 = jro_randint(k_clone, 0, K - 1);
+    if (c0 >= w0) c0 += 1;
+    worst[0] = w0;
+    clone[0] = c0;
+    walk[0] = w0;
+    /* extras (nested_sampling.py:112-133): stable argsort of -noise */
+    if (n_extra > 0) {
+      float* nz = (float*)malloc(sizeof(float) * K);
+      for (int k = 0; k < K; ++k) nz[k] = jro_uniform(jro_bits32(k_extra, (uint32_t)k), 0.0f, 1.0f);
+      nz[w0] = -INFINITY;
+      nz[c0] = -INFINITY;
+      char* used = (char*)calloc(K, 1);
+      for (int e = 0; e < n_extra; ++e) {
+        int bi = -1;
+        for (int k = 0; k < K; ++k)
+          if (!used[k] && (bi < 0 || nz[k] > nz[bi])) bi = k;
+        used[bi] = 1;
+        walk[1 + e] = bi;
+      }
+      free(used);
+      free(nz);
+    }
+  } else {
+    /* _select_culls n_cull > 1 (nested_sampling.py:195-212): order =
+     * lexsort((-noise, -E)); worst = order[:n_cull]; survivors =
+     * permutation(key_clone, order[n_cull:]); clone = survivors[:n_cull];
+     * extras = survivors[n_cull:n_cull + n_extra]. */
+    float* nz = (float*)malloc(sizeof(float) * K);
+    int32_t* order = (int32_t*)malloc(sizeof(int32_t) * K);
+    for (int k = 0; k < K; ++k) nz[k] = jro_uniform(jro_bits32(k_worst, (uint32_t)k), 0.0f, 1.0f);
+    for (int k = 0; k < K; ++k) {
+      int r = 0;
+      for (int j = 0; j < K; ++j)
+        if (j != k && cull_before(rep->energy, nz, j, k)) ++r;
+      order[r] = k;
+    }
+    for (int c = 0; c < n_cull; ++c) worst[c] = order[c];
+    emax = rep->energy[worst[n_cull - 1]];
+    jax_shuffle(k_clone, order + n_cull, K - n_cull);
+    for (int c = 0; c < n_cull; ++c) {
+      clone[c] = order[n_cull + c];
+      walk[c] = worst[c];
+    }
+    for (int e = 0; e < n_extra; ++e) walk[n_cull + e] = order[2 * n_cull + e];
     free(nz);
+    free(order);
   }
-  /* dead walker + evidence (nested_sampling.py:486-501) */
-  double dead_E = rep->energy[worst];
-  if (dead_x) memcpy(dead_x, rep->positions + (size_t)worst * 3 * N, sizeof(float) * 3 * N);
-  if (dead_t) memcpy(dead_t, rep->types + (size_t)worst * N, sizeof(int32_t) * N);
-  if (dead_c) memcpy(dead_c, rep->cell + (size_t)worst * 9, sizeof(float) * 9);
-  double lw = (double)(*rep->iteration) * log_alpha + w_offset;
-  *rep->log_evidence = logaddexp(*rep->log_evidence, lw - dead_E);
-  /* clone into the culled slot, counters reset (nested_sampling.py:504-518) */
-  copy_walker(rep, worst, clone, M);
-  for (int m = 0; m < M; ++m) {
-    rep->n_acc[(size_t)worst * M + m] = 0;
-    rep->n_prop[(size_t)worst * M + m] = 0;
+  /* dead walkers + evidence (nested_sampling.py:486-501) */
+  double* lw = (double*)malloc(sizeof(double) * n_cull);
+  for (int c = 0; c < n_cull; ++c) {
+    const int wc = worst[c];
+    const double dE = rep->energy[wc];
+    if (dead_E_out) dead_E_out[c] = dE;
+    if (dead_x) memcpy(dead_x + (size_t)c * 3 * N, rep->positions + (size_t)wc * 3 * N, sizeof(float) * 3 * N);
+    if (dead_t) memcpy(dead_t + (size_t)c * N, rep->types + (size_t)wc * N, sizeof(int32_t) * N);
+    if (dead_c) memcpy(dead_c + (size_t)c * 9, rep->cell + (size_t)wc * 9, sizeof(float) * 9);
+    lw[c] = (double)(*rep->iteration) * log_alpha + w_offsets[c] - dE;
+  }
+  const double dead_E0 = rep->energy[worst[0]];
+  *rep->log_evidence = n_cull == 1 ? logaddexp(*rep->log_evidence, lw[0])
+                                   : logaddexp(*rep->log_evidence, logsumexp_d(lw, n_cull));
+  free(lw);
+  /* clones into the culled slots, counters reset (nested_sampling.py:504-518) */
+  for (int c = 0; c < n_cull; ++c) {
+    copy_walker(rep, worst[c], clone[c], M);
+    for (int m = 0; m < M; ++m) {
+      rep->n_acc[(size_t)worst[c] * M + m] = 0;
+      rep->n_prop[(size_t)worst[c] * M + m] = 0;
+    }
   }
   memset(info, 0, sizeof(*info));
-  info->worst_idx = worst;
-  info->clone_idx = clone;
+  info->worst_idx = worst[0];
+  info->clone_idx = clone[0];
   info->emax = emax;
-  info->dead_energy = dead_E;
+  info->dead_energy = dead_E0;
+  if (worst_out) memcpy(worst_out, worst, sizeof(int) * n_cull);
+  if (clone_out) memcpy(clone_out, clone, sizeof(int) * n_cull);
   /* walk W chains of T steps (nested_sampling.py:524-628) */
   for (int w = 0; w < W; ++w) {
     uint32_t ck[2];
@@ -1035,11 +1126,22 @@ void jro_ns_step(const JroModel* mdl, const JroMoves* mv, int32_t mode,
       info->total_accepted += acc;
     }
   }
+  free(worst);
+  free(clone);
   free(walk);
   *rep->emax = emax;
   *rep->iteration += 1;
   rep->rng_key[0] = k_next[0];
   rep->rng_key[1] = k_next[1];
+}
+
+void jro_ns_step(const JroModel* mdl, const JroMoves* mv, int32_t mode,
+                 JroReplica* rep, int32_t T, int32_t n_extra,
+                 const uint32_t* move_key_in, double log_alpha, double w_offset,
+                 JroIterInfo* info, float* dead_x, int32_t* dead_t,
+                 float* dead_c) {
+  jro_ns_step_n(mdl, mv, mode, rep, T, 1, n_extra, move_key_in, log_alpha, &w_offset, info,
+                NULL, NULL, NULL, dead_x, dead_t, dead_c);
 }
 
 typedef struct {

@@ -153,6 +153,16 @@ void jro_ns_step(const JroModel* mdl, const JroMoves* mv, int32_t mode,
                  double log_alpha, double w_offset, JroIterInfo* info,
                  float* dead_positions, int32_t* dead_types, float* dead_cell);
 
+/* ns_step with any n_cull (>= 1): worst/clone [n_cull] indices, dead
+ * energies [n_cull], dead walkers [n_cull][...]; w_offsets [n_cull].  Any
+ * output may be NULL. */
+void jro_ns_step_n(const JroModel* mdl, const JroMoves* mv, int32_t mode,
+                   JroReplica* rep, int32_t n_mcmc_steps, int32_t n_cull,
+                   int32_t n_extra, const uint32_t* move_key, double log_alpha,
+                   const double* w_offsets, JroIterInfo* info, int32_t* worst_out,
+                   int32_t* clone_out, double* dead_energy_out, float* dead_positions,
+                   int32_t* dead_types, float* dead_cell);
+
 void jro_re_step(JroReplica* reps, int32_t n_reps, const uint32_t key[2],
                  int32_t n_swap_cycles, int32_t mode, int32_t* acc_per_pair,
                  int32_t* att_per_pair);

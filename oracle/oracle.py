@@ -141,6 +141,11 @@ def lib():
             C.POINTER(JroReplica), C.c_int32, C.c_int32, _u, C.c_double,
             C.c_double, C.POINTER(JroIterInfo), _f, _i, _f,
         ]
+        L.jro_ns_step_n.argtypes = [
+            C.POINTER(JroModel), C.POINTER(JroMoves), C.c_int32,
+            C.POINTER(JroReplica), C.c_int32, C.c_int32, C.c_int32, _u, C.c_double,
+            _d, C.POINTER(JroIterInfo), _i, _i, _d, _f, _i, _f,
+        ]
         L.jro_ns_step_batched.argtypes = [
             C.POINTER(JroModel), C.POINTER(JroMoves), C.c_int32,
             C.POINTER(JroReplica), C.c_int32, C.c_int32, C.c_int32, C.c_int32,
@@ -348,6 +353,29 @@ def ns_step(model, moves, rep: Replica, n_mcmc_steps, log_alpha, w_offset,
         C.byref(info), _p(dx, _f), _p(dt, _i), _p(dc, _f),
     )
     return info, dx, dt, dc
+
+
+def ns_step_n(model, moves, rep: Replica, n_mcmc_steps, log_alpha, w_offsets, n_cull,
+              n_extra=0, move_key=None, mode=DEV):
+    """ns_step with n_cull culls: returns (info, worst, clone, dead_energy,
+    dead_positions, dead_types, dead_cell) with a leading (n_cull,) axis."""
+    info = JroIterInfo()
+    K, N, _ = rep.positions.shape
+    wo = np.ascontiguousarray(np.broadcast_to(np.asarray(w_offsets, np.float64), (n_cull,)))
+    worst = np.zeros(n_cull, np.int32)
+    clone = np.zeros(n_cull, np.int32)
+    de = np.zeros(n_cull, np.float64)
+    dx = np.zeros((n_cull, N, 3), np.float32)
+    dt = np.zeros((n_cull, N), np.int32)
+    dc = np.zeros((n_cull, 3, 3), np.float32)
+    cs = rep.cstruct()
+    mk = None if move_key is None else np.ascontiguousarray(move_key, np.uint32)
+    lib().jro_ns_step_n(
+        C.byref(model), C.byref(moves), mode, C.byref(cs), n_mcmc_steps, n_cull, n_extra,
+        _p(mk, _u) if mk is not None else None, log_alpha, _p(wo, _d), C.byref(info),
+        _p(worst, _i), _p(clone, _i), _p(de, _d), _p(dx, _f), _p(dt, _i), _p(dc, _f),
+    )
+    return info, worst, clone, de, dx, dt, dc
 
 
 def ns_step_batched(model, moves, reps, n_mcmc_steps, log_alpha, w_offset,

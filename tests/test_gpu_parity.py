@@ -207,6 +207,53 @@ def test_supercell_images_match_oracle():
     _compare(case, ns, infos, reps, hist)
 
 
+@pytest.mark.parametrize("P,n_cull,n_extra", [(1, 3, 0), (1, 4, 2), (2, 2, 1)])
+def test_multi_cull_matches_oracle(P, n_cull, n_extra):
+    """n_cull > 1 (nested_sampling.py:195-212): lexsort cull order, permuted
+    survivors as clone sources and extras, per-cull dead points, logsumexp
+    evidence -- walkers, keys and per-cull info identical to the oracle."""
+    case = lj_case(P=P, K=24, N=8, seed=40 + n_cull, n_reflect=3, T=3,
+                   pressure=np.linspace(0.05, 0.3, P))
+    K, T, n_iter = 24, 3, 8
+    batched = P > 1
+    if batched:
+        ns = nsm.init_ns_parallel(case["init_fn"], case["positions"], case["types"],
+                                  case["energies"], case["cells"], case["run_keys"],
+                                  ensemble_params={"pressure": case["pressures"],
+                                                   "chemical_potentials": case["mus"]})
+    else:
+        ns = nsm.init_ns(case["init_fn"], case["positions"][0], case["types"][0],
+                         case["energies"][0], case["cells"][0], case["run_keys"][0],
+                         ensemble_params={"pressure": float(case["pressures"][0])})
+    info = nsm.ns_iterate(ns, case["step"], n_iter, T, n_extra, n_cull=n_cull)
+    torch.cuda.synchronize()
+    reps = oracle_replicas(case)
+    la = prior_mass.log_alpha(K, n_cull)
+    wo = prior_mass.iteration_offsets(K, n_cull)[1]
+    for it in range(n_iter):
+        mk = O.fold_in(reps[0].rng_key, 1) if batched else None
+        for r, rep in enumerate(reps):
+            oi, worst, clone, de, dx, dt, dc = O.ns_step_n(
+                case["model"], case["moves"], rep, T, la, wo, n_cull, n_extra=n_extra,
+                move_key=mk)
+            np.testing.assert_array_equal(_np(info.worst_idx)[it, r], worst)
+            np.testing.assert_array_equal(_np(info.clone_idx)[it, r], clone)
+            np.testing.assert_allclose(_np(info.dead_energy)[it, r], de, rtol=1e-12, atol=0)
+            np.testing.assert_array_equal(_np(info.dead_positions)[it, r], dx)
+            assert abs(float(_np(info.emax)[it, r]) - oi.emax) <= 1e-12 * max(1, abs(oi.emax))
+            lz = float(rep.log_evidence[0])
+            assert abs(float(_np(info.log_evidence)[it, r]) - lz) <= 1e-12 * max(1, abs(lz))
+            np.testing.assert_array_equal(_np(info.n_proposed)[it, r],
+                                          list(oi.n_prop)[:case["step"].n_moves])
+    pop = ns.population
+    for r, rep in enumerate(reps):
+        n = case["Ns"][r]
+        np.testing.assert_array_equal(_np(pop.positions)[r, :, :n], rep.positions)
+        np.testing.assert_array_equal(_np(pop.types)[r, :, :n], rep.types)
+        np.testing.assert_allclose(_np(pop.energy64)[r], rep.energy, rtol=1e-12, atol=0)
+        np.testing.assert_array_equal(_np(ns.rng_key).view(np.uint32)[r], rep.rng_key)
+
+
 @pytest.mark.parametrize("cfg", [(128, 4, 1, 0), (256, 8, 2, 0), (256, 16, 4, 0),
                                  (512, 32, 8, 0), (256, 8, 12, 0), (32, 2, 1, 1),
                                  (128, 2, 1, 1), (64, 2, 4, 1), (128, 2, 8, 1),

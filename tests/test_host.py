@@ -66,15 +66,20 @@ int main(void) {
 
 def test_invalid_arguments_fail_loudly_without_a_gpu():
     L = _lib.load()
-    d = _lib.JrDims(1, 16, 8, 2, 4, 0, 2, 0)  # n_cull = 2 is outside this build
+    d = _lib.JrDims(1, 16, 8, 2, 4, 0, 0, 0)  # n_cull = 0 is out of range
     p = _lib.JrParams()
     p.model.n_species = 1
     p.model.n_images = 1
     p.moves.n_moves = 2
     rc = L.jr_ns_iterate(C.byref(d), C.byref(p), C.byref(_lib.JrStateBuffers()), None, 1,
                          None, None, 0, None)
-    assert rc == -6
+    assert _lib.ERRORS[rc] == "JR_ERR_SHAPE"
     assert b"n_cull" in L.jr_last_error()
+    d.n_cull = 9  # 2 * n_cull + n_extra > n_walkers (the reference's own bound)
+    rc = L.jr_ns_iterate(C.byref(d), C.byref(p), C.byref(_lib.JrStateBuffers()), None, 1,
+                         None, None, 0, None)
+    assert _lib.ERRORS[rc] == "JR_ERR_SHAPE"
+    assert b"2*n_cull" in L.jr_last_error()
     with pytest.raises(_lib.JrError):
         _lib.check(rc, "jr_ns_iterate")
 
@@ -191,3 +196,30 @@ def test_host_prng_matches_oracle():
     assert np.array_equal(prng.split(k, 9), O.split(k, 9))
     assert np.array_equal(prng.fold_in(k, 1), O.fold_in(k, 1))
     assert np.array_equal(prng.advance_iteration(k), O.split(O.split(k, 2)[0], 5)[0])
+
+
+def test_oracle_multi_cull_invariants():
+    """n_cull > 1 (nested_sampling.py:195-212): the culls are the n_cull
+    highest energies in descending order, the contour is the last of them,
+    clone sources and extras are distinct survivors, log Z only grows."""
+    from tests._cases import lj_case, oracle_replicas
+
+    K, nc, nx = 20, 3, 2
+    case = lj_case(P=1, K=K, N=6, seed=15, n_reflect=2, T=2)
+    rep = oracle_replicas(case)[0]
+    la = prior_mass.log_alpha(K, nc)
+    wo = prior_mass.iteration_offsets(K, nc)[1]
+    last = -np.inf
+    for _ in range(12):
+        E = rep.energy.copy()
+        info, worst, clone, de, *_ = O.ns_step_n(case["model"], case["moves"], rep, 2, la, wo,
+                                                 nc, n_extra=nx)
+        top = np.sort(E)[::-1][:nc]
+        np.testing.assert_array_equal(E[worst], top)
+        np.testing.assert_array_equal(de, top)
+        assert info.emax == top[-1]
+        assert len(set(clone.tolist())) == nc and not set(clone.tolist()) & set(worst.tolist())
+        assert sum(info.n_prop) == 2 * (nc + nx)
+        assert rep.log_evidence[0] >= last
+        last = rep.log_evidence[0]
+        assert rep.energy.max() <= info.emax

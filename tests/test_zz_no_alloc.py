@@ -100,10 +100,10 @@ def test_static_scratch_entry_rejects_invalid_dims():
                    pressure=np.array([0.1, 0.2]))
     ns = _init(case)
     dims = nsm.make_dims(ns, case["step"], 2, 0, 1)
-    dims.n_cull = 2
+    dims.n_cull = 0
     params = case["step"].with_evidence(prior_mass.log_alpha(16, 1), 0.0)
     rc = _lib.load().jr_ns_iterate_static(C.byref(dims), C.byref(params),
                                           C.byref(nsm.state_buffers(ns)), None, 1, None,
                                           torch.cuda.current_stream().cuda_stream)
-    assert _lib.ERRORS[rc] == "JR_ERR_UNSUPPORTED"
+    assert _lib.ERRORS[rc] == "JR_ERR_SHAPE"
     assert b"n_cull" in _lib.load().jr_last_error()
