@@ -147,6 +147,31 @@ def fp32_peak_tflops(torch) -> float:
     return best
 
 
+def rank_seed(seed: int, rank: int) -> int:
+    """Each rank owns its own P runs (replicas only: no data-path exchange),
+    seeded apart so no two ranks walk the same runs."""
+    return seed + 1000 * rank
+
+
+def max_over_ranks(ms: float, world: int, device) -> float:
+    """The job's time is the slowest rank's device time."""
+    if world == 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world: int, iters: int, total_ms: float) -> tuple[float, float]:
+    """Whole-job walker-steps/s and NS iterations/s: every rank's P runs,
+    (n_cull + n_extra) * n_mcmc_steps walker-steps per run iteration."""
+    walker_steps = world * P_RUNS * 1 * T * iters
+    return walker_steps / (total_ms * 1e-3), world * P_RUNS * iters / (total_ms * 1e-3)
+
+
 def algorithmic_flops(info) -> float:
     """Sum over the launch's committed iterations of eval counts x unique
     pairs x flops per pair (61 energy+forces, 48 energy-only)."""
@@ -172,7 +197,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     dev = torch.device("cuda", local)
 
-    H, init_fn, step, pos, cells, types, run_keys, re_key = build_case(args.seed + 1000 * rank)
+    H, init_fn, step, pos, cells, types, run_keys, re_key = build_case(rank_seed(args.seed, rank))
     pr = {"pressure": PRESSURES}
     ns = nsm.init_ns_parallel(init_fn, pos, types, None, cells, run_keys, ensemble_params=pr)
     re = nsm.InterREManager(RE_INTERVAL, 1, re_key)
@@ -233,13 +258,8 @@ def run_ours(args):
     total_ms = float(sum(step_ms))
     iters = int((ns.iteration - it_start)[0].item())
     assert iters == args.steps * RE_INTERVAL
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    walker_steps = world * P_RUNS * 1 * T * iters
-    value = walker_steps / (total_ms * 1e-3)
-    ns_iters = world * P_RUNS * iters / (total_ms * 1e-3)
+    total_ms = max_over_ranks(total_ms, world, dev)
+    value, ns_iters = job_throughput(world, iters, total_ms)
     achieved = flops / (sum(kern_ms) * 1e-3) / 1e12
     peak = fp32_peak_tflops(torch)
 
