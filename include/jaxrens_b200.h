@@ -15,7 +15,7 @@
  *   jr_move_trial      <- per_move_fns[k] (src/jaxrens/sampling/mwg.py:152-154),
  *                         used by adjust_step_size
  *                         (src/jaxrens/sampling/adaptation/stepsize_handler.py:246-255)
- *                         and the burn-in walk (src/jaxrens/init/burn_in.py:48-151)
+ *   jr_walk_population <- _one_walk of the burn-in (src/jaxrens/init/burn_in.py:48-127)
  *   jr_energy_forces   <- eval_energy_and_forces on Hamiltonian(LJBackend, EnsembleTerm)
  *                         (src/jaxrens/backends/base.py:74-113,
  *                          src/jaxrens/backends/hamiltonian.py:112-153,
@@ -196,6 +196,18 @@ int jr_ns_iterate(const JrDims* dims, const JrParams* params,
 int jr_ns_iterate_static(const JrDims* dims, const JrParams* params,
                          const JrStateBuffers* state, const JrInfoBuffers* info,
                          int32_t n_iter, const JrLaunchConfig* cfg, void* stream);
+
+/* ---- burn-in walk of the whole population (replaces _one_walk,
+ * src/jaxrens/init/burn_in.py:48-127, called by initial_walk :151-460) ----
+ * Every walker k of every run p takes `walklength` MWG steps under the fixed
+ * contour emax[p]: chain keys split(split(run_keys[p], K)[k], walklength),
+ * move schedule split(move_key, walklength) shared by all walkers and runs.
+ * Walkers keep their own step sizes; their acceptance counters advance.
+ * run_keys [P][2], move_key [2], emax [P] (device). */
+int jr_walk_population(const JrDims* dims, const JrParams* params,
+                       const JrStateBuffers* state, int32_t walklength,
+                       const uint32_t* run_keys, const uint32_t* move_key,
+                       const double* emax, void* stream);
 
 /* ---- one move per (replica, trial) walker (adaptation / burn-in) ---- */
 /* walker_idx [P][n_trials], keys [P][n_trials][2], step [P], emax [P];

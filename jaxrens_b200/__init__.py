@@ -18,6 +18,8 @@ from .backends import (
     eval_energy_and_forces,
 )
 from .moves import MoveKernel, alchemical, galilean, gmc, morph_move, swap, swap_move, volume, volume_move
+from .adaptation import adjust_step_size, build_adapt_step, process_rate
+from .burn_in import initial_walk, walk_population
 from .mwg import build_mwg
 from .nested_sampling import (
     InterREManager,
@@ -40,5 +42,6 @@ __all__ = [
     "morph_move", "swap", "swap_move", "volume", "volume_move", "build_mwg",
     "InterREManager", "IterationTermination", "NSState", "PriorMassTermination",
     "final_log_evidence", "init_ns", "init_ns_parallel", "ns_iterate", "ns_step",
-    "run_loop", "run_ns", "run_ns_parallel",
+    "run_loop", "run_ns", "run_ns_parallel", "adjust_step_size", "build_adapt_step",
+    "process_rate", "initial_walk", "walk_population",
 ]

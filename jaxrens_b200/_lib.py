@@ -136,6 +136,7 @@ EXPORTED = (
     "jr_ns_iterate",
     "jr_ns_iterate_static",
     "jr_move_trial",
+    "jr_walk_population",
     "jr_energy_forces",
     "jr_re_swap",
     "jr_autotune",
@@ -188,6 +189,10 @@ def load():
     L.jr_move_trial.argtypes = [
         P(JrDims), P(JrParams), P(JrStateBuffers), C.c_int32, C.c_int32, _vp, _vp,
         _vp, _vp, _vp, C.c_int32, _vp, _vp, _vp,
+    ]
+    L.jr_walk_population.restype = C.c_int
+    L.jr_walk_population.argtypes = [
+        P(JrDims), P(JrParams), P(JrStateBuffers), C.c_int32, _vp, _vp, _vp, _vp,
     ]
     L.jr_energy_forces.restype = C.c_int
     L.jr_energy_forces.argtypes = [

@@ -620,6 +620,52 @@ move_trial_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st, co
   if (write_back) store_walker(D, st, w, p, slot);
 }
 
+// ------------------------------------------------------- burn-in walk ----
+// _one_walk (init/burn_in.py:48-127): every walker k of every run p takes
+// `walklength` MWG steps under the fixed contour emax[p], chain keys
+// split(split(run_key[p], K)[k], walklength) and the move schedule
+// split(move_key, walklength) shared by every walker and run; step sizes
+// are the walker's own and its acceptance counters advance.  One group per
+// walker, walkers of one CTA may belong to different runs.
+template <class G, int kMaxThreads>
+__global__ void __launch_bounds__(kMaxThreads, 1)
+walk_population_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
+                       const int walklength, const uint32_t* run_keys,
+                       const uint32_t* move_key, const double* emax, const int tpa) {
+  constexpr bool kWarp = std::is_same<G, WarpGroup>::value;
+  extern __shared__ __align__(16) unsigned char dyn[];
+  __shared__ JrParams P;
+  __shared__ PairTables tab;
+  __shared__ double red[2][kMaxWarps][3];
+  copy_params(P, Pg);
+  const int gpc = kWarp ? (int)(blockDim.x >> 5) : 1;
+  const int my = kWarp ? (int)(threadIdx.x >> 5) : 0;
+  const int K = D.n_walkers;
+  const int total = D.n_replicas * K;
+  const int t_global = blockIdx.x * gpc + my;
+  const int nimg = Pg.model.n_images;
+  const size_t ptb = pair_table_bytes(D.n_atoms_max, nimg);
+  char* base = reinterpret_cast<char*>(dyn) +
+               (size_t)my * (ptb + walker_smem_bytes(D.n_atoms_max, nimg));
+  uint16_t* pij = ptb ? reinterpret_cast<uint16_t*>(base) : nullptr;
+  WalkArrays arr;
+  WalkShared* wsp = carve_walker(base + ptb, D.n_atoms_max, nimg, pij, arr);
+  __syncthreads();
+  load_tables(P, tab);
+  __syncthreads();
+  if (t_global >= total) return;  // whole group leaves together
+  const int p = t_global / K, slot = t_global % K;
+  const int n = min(max(st.n_atoms[p], 1), D.n_atoms_max);
+  Walker<G> w{*wsp, arr, tab, n, tpa, make_group<G>(red), 0};
+  build_group_pair_table(w.g, pij, n);
+  load_walker(P, D, st, w, p, slot, false);
+  const float* mu = st.mu ? st.mu + (size_t)p * P.model.n_species : nullptr;
+  const Key rk{run_keys[2 * p], run_keys[2 * p + 1]};
+  const Key mk{move_key[0], move_key[1]};
+  walk_chain(P, w, walklength, split(rk, (uint32_t)slot), mk, emax[p], st.pressure[p], mu);
+  store_walker(D, st, w, p, slot);
+}
+
 // ------------------------------------------------------------ energy ----
 template <class G, int kMaxThreads>
 __global__ void __launch_bounds__(kMaxThreads, 1)
@@ -1117,6 +1163,40 @@ int jr_move_trial(const JrDims* dims, const JrParams* params, const JrStateBuffe
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "move_trial launch");
+  return JR_OK;
+}
+
+int jr_walk_population(const JrDims* dims, const JrParams* params, const JrStateBuffers* state,
+                       int32_t walklength, const uint32_t* run_keys, const uint32_t* move_key,
+                       const double* emax, void* stream) {
+  int rc = check_params(dims, params);
+  if (rc) return rc;
+  if (!state || !run_keys || !move_key || !emax || walklength < 0)
+    return fail(JR_ERR_PARAM, "walk_population: null buffer or walklength < 0");
+  if (walklength == 0) return JR_OK;
+  const JrLaunchConfig c = heuristic_config(dims);
+  const int nimg = params->model.n_images;
+  const int total = dims->n_replicas * dims->n_walkers;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e;
+  if (c.warp_walkers) {
+    const int gpc = c.threads / 32;
+    const size_t smem = group_dyn_smem(dims->n_atoms_max, nimg, gpc);
+    e = cudaFuncSetAttribute(jr::walk_population_kernel<jr::WarpGroup, 128>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "smem attribute");
+    jr::walk_population_kernel<jr::WarpGroup, 128><<<(total + gpc - 1) / gpc, c.threads, smem, s>>>(
+        *dims, *params, *state, walklength, run_keys, move_key, emax, c.tpa);
+  } else {
+    const size_t smem = group_dyn_smem(dims->n_atoms_max, nimg, 1);
+    e = cudaFuncSetAttribute(jr::walk_population_kernel<jr::CtaGroup, 512>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "smem attribute");
+    jr::walk_population_kernel<jr::CtaGroup, 512><<<total, c.threads, smem, s>>>(
+        *dims, *params, *state, walklength, run_keys, move_key, emax, c.tpa);
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "walk_population launch");
   return JR_OK;
 }
 

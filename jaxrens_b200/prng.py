@@ -77,3 +77,19 @@ def uniform(k, n: int) -> np.ndarray:
 def advance_iteration(k) -> np.ndarray:
     """The run key after one ns_step iteration (nested_sampling.py:465-466)."""
     return split(split(k, 2)[0], 5)[0]
+
+
+def randint_array(k, n: int, lo: int, hi: int) -> np.ndarray:
+    """``jax.random.randint(k, (n,), lo, hi)`` int32: with ``k1, k2 =
+    split(k)``, element i combines ``higher = bits(k1)[i]`` and ``lower =
+    bits(k2)[i]`` as ``((higher % span) * m + lower % span) % span`` in
+    wrapping uint32 arithmetic, ``m = (2**16 % span)**2 % span``."""
+    k1, k2 = split(k, 2)
+    higher = random_bits(k1, n)
+    lower = random_bits(k2, n)
+    span = np.uint32(max(int(hi) - int(lo), 1))
+    mult = np.uint32(65536 % int(span))
+    mult = np.uint32((int(mult) * int(mult)) % int(span))
+    with np.errstate(over="ignore"):
+        off = ((higher % span) * mult + (lower % span)) % span
+    return (np.int64(lo) + off.astype(np.int64)).astype(np.int32)

@@ -1144,6 +1144,34 @@ void jro_ns_step(const JroModel* mdl, const JroMoves* mv, int32_t mode,
                 NULL, NULL, NULL, dead_x, dead_t, dead_c);
 }
 
+/* _one_walk (init/burn_in.py:48-127) for one run: walker k takes walklength
+ * MWG steps under the fixed contour emax with chain keys
+ * split(split(run_key, K)[k], walklength) and the shared move schedule
+ * split(move_key, walklength); its own step sizes, counters advanced. */
+void jro_walk_population(const JroModel* mdl, const JroMoves* mv, int32_t mode,
+                         JroReplica* rep, int32_t walklength, const uint32_t run_key[2],
+                         const uint32_t move_key[2], double emax) {
+  const int K = rep->n_walkers, N = rep->n_atoms, M = mv->n_moves;
+  for (int k = 0; k < K; ++k) {
+    uint32_t ck[2];
+    jro_split(run_key, (uint32_t)k, ck);
+    float* x = rep->positions + (size_t)k * 3 * N;
+    float* d = rep->direction + (size_t)k * 3 * N;
+    int32_t* t = rep->types + (size_t)k * N;
+    float* c = rep->cell + (size_t)k * 9;
+    for (int step = 0; step < walklength; ++step) {
+      uint32_t sk[2], mk[2];
+      jro_split(ck, (uint32_t)step, sk);
+      jro_split(move_key, (uint32_t)step, mk);
+      int midx, reason, ne, ng;
+      jro_mwg_step(mdl, mv, mode, sk, mk, emax, N, x, d, t, c, &rep->energy[k],
+                   rep->step_sizes + (size_t)k * M, rep->n_acc + (size_t)k * M,
+                   rep->n_prop + (size_t)k * M, rep->pressure, rep->mu, rep->has_mu,
+                   &midx, &reason, &ne, &ng);
+    }
+  }
+}
+
 typedef struct {
   const JroModel* mdl; const JroMoves* mv; int32_t mode; JroReplica* reps;
   int32_t n_reps, T, n_extra; const uint32_t* mk; double log_alpha, w_offset;

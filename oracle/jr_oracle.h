@@ -163,6 +163,11 @@ void jro_ns_step_n(const JroModel* mdl, const JroMoves* mv, int32_t mode,
                    int32_t* clone_out, double* dead_energy_out, float* dead_positions,
                    int32_t* dead_types, float* dead_cell);
 
+/* Burn-in walk of every walker of one run (init/burn_in.py _one_walk). */
+void jro_walk_population(const JroModel* mdl, const JroMoves* mv, int32_t mode,
+                         JroReplica* rep, int32_t walklength, const uint32_t run_key[2],
+                         const uint32_t move_key[2], double emax);
+
 void jro_re_step(JroReplica* reps, int32_t n_reps, const uint32_t key[2],
                  int32_t n_swap_cycles, int32_t mode, int32_t* acc_per_pair,
                  int32_t* att_per_pair);

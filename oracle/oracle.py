@@ -146,6 +146,10 @@ def lib():
             C.POINTER(JroReplica), C.c_int32, C.c_int32, C.c_int32, _u, C.c_double,
             _d, C.POINTER(JroIterInfo), _i, _i, _d, _f, _i, _f,
         ]
+        L.jro_walk_population.argtypes = [
+            C.POINTER(JroModel), C.POINTER(JroMoves), C.c_int32, C.POINTER(JroReplica),
+            C.c_int32, _u, _u, C.c_double,
+        ]
         L.jro_ns_step_batched.argtypes = [
             C.POINTER(JroModel), C.POINTER(JroMoves), C.c_int32,
             C.POINTER(JroReplica), C.c_int32, C.c_int32, C.c_int32, C.c_int32,
@@ -376,6 +380,16 @@ def ns_step_n(model, moves, rep: Replica, n_mcmc_steps, log_alpha, w_offsets, n_
         _p(worst, _i), _p(clone, _i), _p(de, _d), _p(dx, _f), _p(dt, _i), _p(dc, _f),
     )
     return info, worst, clone, de, dx, dt, dc
+
+
+def walk_population(model, moves, rep: Replica, walklength, run_key, move_key, emax,
+                    mode=DEV):
+    """Burn-in walk of every walker of one run, in place."""
+    cs = rep.cstruct()
+    rk = np.ascontiguousarray(run_key, np.uint32)
+    mk = np.ascontiguousarray(move_key, np.uint32)
+    lib().jro_walk_population(C.byref(model), C.byref(moves), mode, C.byref(cs), int(walklength),
+                              _p(rk, _u), _p(mk, _u), float(emax))
 
 
 def ns_step_batched(model, moves, reps, n_mcmc_steps, log_alpha, w_offset,
