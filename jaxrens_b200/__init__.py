@@ -20,6 +20,7 @@ from .backends import (
 from .moves import MoveKernel, alchemical, galilean, gmc, morph_move, swap, swap_move, volume, volume_move
 from .adaptation import adjust_step_size, build_adapt_step, process_rate
 from .burn_in import initial_walk, walk_population
+from .energy_log import EnergyLogCallback, EnergyLogger
 from .mwg import build_mwg
 from .nested_sampling import (
     InterREManager,
@@ -43,5 +44,5 @@ __all__ = [
     "InterREManager", "IterationTermination", "NSState", "PriorMassTermination",
     "final_log_evidence", "init_ns", "init_ns_parallel", "ns_iterate", "ns_step",
     "run_loop", "run_ns", "run_ns_parallel", "adjust_step_size", "build_adapt_step",
-    "process_rate", "initial_walk", "walk_population",
+    "process_rate", "initial_walk", "walk_population", "EnergyLogCallback", "EnergyLogger",
 ]

@@ -526,6 +526,7 @@ def run_loop(ns_state: NSState, step_fn: MWGStep, n_mcmc_steps: int, n_extra: in
         lz = info.log_evidence.cpu().numpy()
         em = info.emax.cpu().numpy()
         stop = False
+        n_keep = chunk
         for r in range(chunk):
             it = i + r
             if inter_re is not None and r == chunk - 1 and inter_re.fires(it):
@@ -545,7 +546,11 @@ def run_loop(ns_state: NSState, step_fn: MWGStep, n_mcmc_steps: int, n_extra: in
                     c.update_evidence(log_z)
             stop, _ = check_any(termination_criteria, it, hmax)
             if stop:
+                n_keep = r + 1
                 break
+        for cb in callbacks:
+            if hasattr(cb, "on_launch"):
+                cb.on_launch(i, info, n_keep)
         i += chunk
         if stop:
             return ns_state
