@@ -109,6 +109,10 @@ typedef struct JrMoveParams {
   float cum_probs[JR_MAX_MOVES];     /* float32 cumsum(w / sum(w)) */
   float max_vpa, min_vpa, min_aspect; /* cell-geometry guard */
   int32_t flat_v_prior;
+  /* minimum-distance constraint gate (constraints/min_distance.py): applied
+   * after move m when gate[m] != 0; dmin is the S x S threshold matrix */
+  int32_t gate[JR_MAX_MOVES];
+  float dmin[JR_MAX_SPECIES * JR_MAX_SPECIES];
 } JrMoveParams;
 
 typedef struct JrParams {

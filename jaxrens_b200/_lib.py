@@ -73,6 +73,8 @@ class JrMoveParams(C.Structure):
         ("min_vpa", C.c_float),
         ("min_aspect", C.c_float),
         ("flat_v_prior", C.c_int32),
+        ("gate", C.c_int32 * MAX_MOVES),
+        ("dmin", C.c_float * (MAX_SPECIES * MAX_SPECIES)),
     ]
 
 

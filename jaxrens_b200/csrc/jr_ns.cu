@@ -607,7 +607,7 @@ move_trial_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st, co
     idx = choice(mk, P.moves.cum_probs, P.moves.n_moves);
   }
   int reason = 0;
-  const bool acc = run_move(P, w, idx, key, step[p], emax[p], st.pressure[p], mu, reason);
+  const bool acc = gated_move(P, w, idx, key, step[p], emax[p], st.pressure[p], mu, reason);
   w.g.sync();
   if (w.g.leader()) {
     accepted[tb] = acc ? 1 : 0;

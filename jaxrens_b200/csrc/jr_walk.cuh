@@ -115,6 +115,10 @@ struct WalkShared {
   int c_rr[JR_MAX_MOVES * 4];
   int c_nev[JR_MAX_MOVES];
   int c_ngr[JR_MAX_MOVES];
+  // pre-move copy for the constraint gate
+  double E_save;
+  int cur_save;
+  int counts_save[JR_MAX_SPECIES];
 };
 
 // Pair tables of the model, shared by every walker of a CTA.
@@ -131,6 +135,7 @@ struct PairTables {
 // atom count).
 struct WalkArrays {
   float4* xs;           // [Nmax] position + type bits (current / trial positions)
+  float4* xsave;        // [Nmax] pre-move copy of xs for the constraint gate
   float* x0;            // [3 Nmax] saved positions
   float* dir;           // [3 Nmax] direction
   float* dp;            // [3 Nmax] perturbed direction (flip target on reject)
@@ -153,7 +158,7 @@ __host__ __device__ inline size_t pair_count(int nmax) {
 // Bytes of one walker: WalkShared + arrays (+ pair buffer).
 __host__ __device__ inline size_t walker_smem_bytes(int nmax, int nimg) {
   size_t b = align16(sizeof(WalkShared));
-  b += 16u * (size_t)nmax + 4u * 12u * (size_t)nmax;
+  b += 2u * 16u * (size_t)nmax + 4u * 12u * (size_t)nmax;
   b += align16(2u * 3u * 4u * (size_t)nimg);
   if (use_pair_matrix(nmax, nimg)) b += align16(12u * (size_t)nmax * (size_t)(nmax | 1));
   return align16(b);
@@ -169,6 +174,7 @@ __device__ inline WalkShared* carve_walker(char* p, int nmax, int nimg, const ui
   WalkShared* s = reinterpret_cast<WalkShared*>(p);
   p += align16(sizeof(WalkShared));
   a.xs = (float4*)p; p += 16 * nmax;
+  a.xsave = (float4*)p; p += 16 * nmax;
   a.x0 = (float*)p; p += 12 * nmax;
   a.dir = (float*)p; p += 12 * nmax;
   a.dp = (float*)p; p += 12 * nmax;
@@ -1060,6 +1066,88 @@ __device__ __forceinline__ bool run_move(const JrParams& P, Walker<G>& w, int id
   return false;
 }
 
+// Minimum-distance constraint (constraints/min_distance.py:25-47 with the
+// MIC of backends/geometry.py:18-69): every pair i != j must be at least
+// dmin[t_i][t_j] apart.  Periodic iff |det(cell)| > 1e-10: fractional
+// coordinates f = x . inv(cell) (float32, FMA order of the pair MIC),
+// df = f_i - f_j - rint(f_i - f_j), delta = df . cell; otherwise the raw
+// difference; the distance is the correctly rounded sqrt of |delta|^2.
+// Group-uniform result.
+template <class G>
+__device__ inline bool min_distance_ok(const JrParams& P, Walker<G>& w) {
+  const CellCtx& cc = w.s.cc[w.s.cur];
+  const bool periodic = cc.vol > 1e-10f;
+  const float4* xs = w.arr.xs;
+  const int n = w.n, S = P.model.n_species;
+  double bad = 0.0;
+  for (int q = w.g.rank(); q < n * n; q += w.g.size()) {
+    const int i = q / n, j = q - i * n;
+    if (j <= i) continue;
+    const float4 a = xs[i], b = xs[j];
+    const float thr = P.moves.dmin[__float_as_int(a.w) * S + __float_as_int(b.w)];
+    float d[3];
+    if (periodic) {
+      float fa[3], fb[3];
+      for (int k = 0; k < 3; ++k) {
+        fa[k] = __fmaf_rn(a.z, cc.inv[6 + k], __fmaf_rn(a.y, cc.inv[3 + k], __fmul_rn(a.x, cc.inv[k])));
+        fb[k] = __fmaf_rn(b.z, cc.inv[6 + k], __fmaf_rn(b.y, cc.inv[3 + k], __fmul_rn(b.x, cc.inv[k])));
+      }
+      float df[3];
+      for (int k = 0; k < 3; ++k) {
+        df[k] = __fsub_rn(fa[k], fb[k]);
+        df[k] = __fsub_rn(df[k], rintf(df[k]));
+      }
+      for (int k = 0; k < 3; ++k)
+        d[k] = __fmaf_rn(df[2], cc.raw[6 + k], __fmaf_rn(df[1], cc.raw[3 + k], __fmul_rn(df[0], cc.raw[k])));
+    } else {
+      d[0] = __fsub_rn(a.x, b.x);
+      d[1] = __fsub_rn(a.y, b.y);
+      d[2] = __fsub_rn(a.z, b.z);
+    }
+    const float r2 = __fmaf_rn(d[2], d[2], __fmaf_rn(d[1], d[1], __fmul_rn(d[0], d[0])));
+    if (__fsqrt_rn(r2) < thr) bad = 1.0;
+  }
+  return group_sum1(w, bad) == 0.0;
+}
+
+// One move through the _wrap gate (mwg.py:108-150): a move that the
+// minimum-distance constraint applies to (gate[idx], set by the host from the
+// move's `mutates` and the constraint's `depends_on`) and that was accepted
+// into a violating configuration is undone -- positions, cell, types and
+// energy back to the pre-move state, the direction kept -- and reports
+// reject reason 4.
+template <class G>
+__device__ __forceinline__ bool gated_move(const JrParams& P, Walker<G>& w, int idx, Key key,
+                                           float step, double emax, float pressure,
+                                           const float* mu, int& reason) {
+  if (!P.moves.gate[idx]) return run_move(P, w, idx, key, step, emax, pressure, mu, reason);
+  WalkShared& s = w.s;
+  const int n = w.n;
+  w.g.sync();
+  for (int i = w.g.rank(); i < n; i += w.g.size()) w.arr.xsave[i] = w.arr.xs[i];
+  if (w.g.leader()) {
+    s.E_save = s.E;
+    s.cur_save = s.cur;
+    for (int q = 0; q < JR_MAX_SPECIES; ++q) s.counts_save[q] = s.counts[q];
+  }
+  w.g.sync();
+  bool acc = run_move(P, w, idx, key, step, emax, pressure, mu, reason);
+  w.g.sync();
+  if (acc && !min_distance_ok(P, w)) {
+    for (int i = w.g.rank(); i < n; i += w.g.size()) w.arr.xs[i] = w.arr.xsave[i];
+    w.g.sync();
+    if (w.g.leader()) {
+      s.E = s.E_save;
+      s.cur = s.cur_save;
+      for (int q = 0; q < JR_MAX_SPECIES; ++q) s.counts[q] = s.counts_save[q];
+    }
+    w.g.sync();
+    acc = false;
+    reason = 4;
+  }
+  return acc;
+}
+
 // MWG step (mwg.py:227-257 with the _wrap counters of mwg.py:108-150) plus
 // the ns_step scan-body counters (nested_sampling.py:541-609).
 template <class G>
@@ -1069,14 +1157,16 @@ __device__ __forceinline__ void mwg_step(const JrParams& P, Walker<G>& w, Key st
   WalkShared& s = w.s;
   const int idx = choice(move_key, P.moves.cum_probs, P.moves.n_moves);
   int reason = 0;
-  const bool acc = run_move(P, w, idx, step_key, s.step_sizes[idx], emax, pressure, mu, reason);
+  const bool acc = gated_move(P, w, idx, step_key, s.step_sizes[idx], emax, pressure, mu, reason);
   if (w.g.leader()) {
     s.w_prop[idx] += 1;
     s.w_acc[idx] += acc ? 1 : 0;
     s.c_prop[idx] += 1;
     s.c_acc[idx] += acc ? 1 : 0;
+    // reason 4 (a constraint) lies outside the 4 buckets: the reference's
+    // scatter drops it (nested_sampling.py:562-570)
     const int col = acc ? 0 : (reason > 1 ? reason : 1);
-    s.c_rr[idx * 4 + col] += 1;
+    if (col < 4) s.c_rr[idx * 4 + col] += 1;
     const bool gal = P.moves.type[idx] == JR_MOVE_GALILEAN;
     const int ne = gal ? P.moves.n_reflect[idx] : 1;
     s.c_nev[idx] += ne;

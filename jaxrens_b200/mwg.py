@@ -73,9 +73,12 @@ def _move_params(specs: list[MoveSpec], probs_cum: np.ndarray) -> _lib.JrMovePar
 
 
 def build_mwg(backend, move_descriptors: list[MoveKernel], constraint_descriptors=()):
-    """Build ``(init_fn, step_fn, per_move_fns)`` (``mwg.py:40-259``)."""
-    if constraint_descriptors:
-        raise NotImplementedError("configuration-constraint gates are not in this build")
+    """Build ``(init_fn, step_fn, per_move_fns)`` (``mwg.py:40-259``).
+    ``constraint_descriptors`` (``constraints.min_distance_descriptor``) gate
+    the moves that can violate them (``mwg.py:97-150``)."""
+    from .constraints import move_gates
+
+    gates, dmin = move_gates(tuple(constraint_descriptors), move_descriptors)
     if not isinstance(backend, Hamiltonian):
         backend = Hamiltonian(backend, [])
     specs = [d.build_kernel(backend, **d.kernel_kwargs) for d in move_descriptors]
@@ -86,6 +89,13 @@ def build_mwg(backend, move_descriptors: list[MoveKernel], constraint_descriptor
     params = _lib.JrParams()
     params.model = backend.model_params()
     params.moves = _move_params(specs, cum)
+    if dmin is not None:
+        S = backend.model_params().n_species
+        if dmin.shape != (S, S):
+            raise ValueError(f"d_min matrix must be ({S}, {S}) for this model")
+        for m, g in enumerate(gates):
+            params.moves.gate[m] = g
+        params.moves.dmin[: S * S] = [float(v) for v in dmin.reshape(-1)]
     defaults = np.array([d.step_size for d in move_descriptors], np.float32)
     step = MWGStep(backend, list(move_descriptors), specs, params, probs, defaults)
 

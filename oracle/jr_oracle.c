@@ -857,12 +857,64 @@ static double round_energy(double e, int mode) {
   return mode == JRO_REF32 ? (double)(float)e : e;
 }
 
+/* Minimum-distance predicate (constraints/min_distance.py:25-47, MIC of
+ * backends/geometry.py:18-69): periodic iff |det(cell)| > 1e-10, fractional
+ * f = x . inv(cell), df = f_i - f_j - rint(f_i - f_j), delta = df . cell
+ * (the pair-MIC FMA order; plain products in REF32), else the raw
+ * difference; violated when sqrt(|delta|^2) < dmin[t_i][t_j], i != j. */
+int32_t jro_min_distance_ok(const JroMoves* mv, int32_t S, int32_t n, const float* x,
+                            const int32_t* t, const float* cell, int32_t mode) {
+  const int periodic = fabsf(jro_det3(cell)) > 1e-10f;
+  float inv[9];
+  if (periodic) jro_inv_cell(cell, inv);
+  for (int i = 0; i < n; ++i)
+    for (int j = i + 1; j < n; ++j) {
+      float dd[3];
+      if (periodic) {
+        float fa[3], fb[3], df[3];
+        for (int k = 0; k < 3; ++k) {
+          if (mode == JRO_REF32) {
+            fa[k] = x[3 * i] * inv[k] + x[3 * i + 1] * inv[3 + k] + x[3 * i + 2] * inv[6 + k];
+            fb[k] = x[3 * j] * inv[k] + x[3 * j + 1] * inv[3 + k] + x[3 * j + 2] * inv[6 + k];
+          } else {
+            fa[k] = fmaf(x[3 * i + 2], inv[6 + k], fmaf(x[3 * i + 1], inv[3 + k], x[3 * i] * inv[k]));
+            fb[k] = fmaf(x[3 * j + 2], inv[6 + k], fmaf(x[3 * j + 1], inv[3 + k], x[3 * j] * inv[k]));
+          }
+          df[k] = fa[k] - fb[k];
+          df[k] = df[k] - rintf(df[k]);
+        }
+        for (int k = 0; k < 3; ++k)
+          dd[k] = mode == JRO_REF32
+                      ? df[0] * cell[k] + df[1] * cell[3 + k] + df[2] * cell[6 + k]
+                      : fmaf(df[2], cell[6 + k], fmaf(df[1], cell[3 + k], df[0] * cell[k]));
+      } else {
+        for (int k = 0; k < 3; ++k) dd[k] = x[3 * i + k] - x[3 * j + k];
+      }
+      const float r2 = mode == JRO_REF32 ? dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]
+                                         : fmaf(dd[2], dd[2], fmaf(dd[1], dd[1], dd[0] * dd[0]));
+      if (sqrtf(r2) < mv->dmin[t[i] * S + t[j]]) return 0;
+    }
+  return 1;
+}
+
 int32_t jro_move_trial(const JroModel* mdl, const JroMoves* mv, int32_t mode,
                        int32_t move_idx, const uint32_t key[2], float step,
                        double emax, int32_t n, float* x, float* d, int32_t* t,
                        float* cell, double* energy, float P, const float* mu,
                        int32_t has_mu, int32_t* reason_out) {
   int reason = 0, acc = 0;
+  const int gated = mv->gate[move_idx] != 0;
+  float* xs = NULL;
+  int32_t* ts = NULL;
+  float cs[9];
+  double es = *energy;
+  if (gated) {
+    xs = (float*)malloc(sizeof(float) * 3 * n);
+    ts = (int32_t*)malloc(sizeof(int32_t) * n);
+    memcpy(xs, x, sizeof(float) * 3 * n);
+    memcpy(ts, t, sizeof(int32_t) * n);
+    memcpy(cs, cell, sizeof(cs));
+  }
   switch (mv->type[move_idx]) {
     case JRO_MOVE_GALILEAN:
       acc = move_galilean(mdl, mode, key, step, mv->n_reflect[move_idx],
@@ -882,6 +934,20 @@ int32_t jro_move_trial(const JroModel* mdl, const JroMoves* mv, int32_t mode,
       break;
   }
   *energy = round_energy(*energy, mode);
+  if (gated) {
+    /* mwg.py _wrap: an accepted violating move is undone (positions, cell,
+     * types, energy; the direction is kept) with reject reason 4 */
+    if (acc && !jro_min_distance_ok(mv, mdl->n_species, n, x, t, cell, mode)) {
+      memcpy(x, xs, sizeof(float) * 3 * n);
+      memcpy(t, ts, sizeof(int32_t) * n);
+      memcpy(cell, cs, sizeof(cs));
+      *energy = es;
+      acc = 0;
+      reason = 4;
+    }
+    free(xs);
+    free(ts);
+  }
   if (reason_out) *reason_out = reason;
   return acc;
 }
@@ -1120,7 +1186,7 @@ void jro_ns_step_n(const JroModel* mdl, const JroMoves* mv, int32_t mode,
       info->n_acc[midx] += acc;
       info->n_prop[midx] += 1;
       int col = acc ? 0 : (reason > 1 ? reason : 1);
-      info->rr[midx * 4 + col] += 1;
+      if (col < 4) info->rr[midx * 4 + col] += 1;  /* reason 4 is dropped */
       info->n_evals[midx] += ne;
       info->n_grad[midx] += ng;
       info->total_accepted += acc;

@@ -70,6 +70,10 @@ typedef struct JroMoves {
   /* cell-move guard (src/jaxrens/utils/cell.py:105-125) */
   float max_vpa, min_vpa, min_aspect;
   int32_t flat_v_prior;
+  /* minimum-distance gate (constraints/min_distance.py, mwg.py:108-150):
+   * applied after move m when gate[m]; dmin is the S x S threshold matrix */
+  int32_t gate[JRO_MAX_MOVES];
+  float dmin[JRO_MAX_SPECIES * JRO_MAX_SPECIES];
 } JroMoves;
 
 /* One replica's population, walker-major, N atoms (no padding). */
@@ -162,6 +166,10 @@ void jro_ns_step_n(const JroModel* mdl, const JroMoves* mv, int32_t mode,
                    const double* w_offsets, JroIterInfo* info, int32_t* worst_out,
                    int32_t* clone_out, double* dead_energy_out, float* dead_positions,
                    int32_t* dead_types, float* dead_cell);
+
+/* Minimum-distance constraint verdict (1 = every pair far enough). */
+int32_t jro_min_distance_ok(const JroMoves* mv, int32_t S, int32_t n, const float* x,
+                            const int32_t* t, const float* cell, int32_t mode);
 
 /* Burn-in walk of every walker of one run (init/burn_in.py _one_walk). */
 void jro_walk_population(const JroModel* mdl, const JroMoves* mv, int32_t mode,

@@ -60,6 +60,8 @@ class JroMoves(C.Structure):
         ("min_vpa", C.c_float),
         ("min_aspect", C.c_float),
         ("flat_v_prior", C.c_int32),
+        ("gate", C.c_int32 * MAX_MOVES),
+        ("dmin", C.c_float * (MAX_SPECIES * MAX_SPECIES)),
     ]
 
 
@@ -146,6 +148,8 @@ def lib():
             C.POINTER(JroReplica), C.c_int32, C.c_int32, C.c_int32, _u, C.c_double,
             _d, C.POINTER(JroIterInfo), _i, _i, _d, _f, _i, _f,
         ]
+        L.jro_min_distance_ok.argtypes = [C.POINTER(JroMoves), C.c_int32, C.c_int32, _f, _i,
+                                          _f, C.c_int32]
         L.jro_walk_population.argtypes = [
             C.POINTER(JroModel), C.POINTER(JroMoves), C.c_int32, C.POINTER(JroReplica),
             C.c_int32, _u, _u, C.c_double,
@@ -261,7 +265,8 @@ def make_model(eps4, eps24, sig2, rc2=None, img_off=None, model=MODEL_LJ,
 
 
 def make_moves(types, n_reflect, perturb_angle, cum_probs, max_vpa=1e4,
-               min_vpa=1.0, min_aspect=0.8, flat_v_prior=False) -> JroMoves:
+               min_vpa=1.0, min_aspect=0.8, flat_v_prior=False, gate=None,
+               dmin=None) -> JroMoves:
     mv = JroMoves()
     M = len(types)
     mv.n_moves = M
@@ -273,6 +278,11 @@ def make_moves(types, n_reflect, perturb_angle, cum_probs, max_vpa=1e4,
     mv.min_vpa = min_vpa
     mv.min_aspect = min_aspect
     mv.flat_v_prior = int(flat_v_prior)
+    if gate is not None:
+        mv.gate[:M] = [int(g) for g in gate]
+    if dmin is not None:
+        dm = np.asarray(dmin, np.float32).reshape(-1)
+        mv.dmin[: dm.size] = dm.tolist()
     return mv
 
 
@@ -380,6 +390,14 @@ def ns_step_n(model, moves, rep: Replica, n_mcmc_steps, log_alpha, w_offsets, n_
         _p(worst, _i), _p(clone, _i), _p(de, _d), _p(dx, _f), _p(dt, _i), _p(dc, _f),
     )
     return info, worst, clone, de, dx, dt, dc
+
+
+def min_distance_ok(moves, n_species, x, types, cell, mode=DEV) -> bool:
+    x = np.ascontiguousarray(x, np.float32).reshape(-1, 3)
+    t = np.ascontiguousarray(types, np.int32)
+    c = np.ascontiguousarray(cell, np.float32).reshape(9)
+    return bool(lib().jro_min_distance_ok(C.byref(moves), n_species, x.shape[0], _p(x, _f),
+                                          _p(t, _i), _p(c, _f), mode))
 
 
 def walk_population(model, moves, rep: Replica, walklength, run_key, move_key, emax,

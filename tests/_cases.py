@@ -26,13 +26,14 @@ def oracle_moves(step) -> O.JroMoves:
     return O.make_moves([p.type[m] for m in range(M)], [p.n_reflect[m] for m in range(M)],
                         [p.perturb_angle[m] for m in range(M)],
                         [p.cum_probs[m] for m in range(M)], p.max_vpa, p.min_vpa,
-                        p.min_aspect, bool(p.flat_v_prior))
+                        p.min_aspect, bool(p.flat_v_prior), [p.gate[m] for m in range(M)],
+                        list(p.dmin))
 
 
 def lj_case(P=1, K=32, N=8, seed=0, n_reflect=4, T=5, pressure=0.1, epsilon=1.0,
             sigma=1.0, cutoff=2.5, supercell=(1, 1, 1), v_hi_per_atom=8.0,
             n_atoms_list=None, mu=None, identity=None, step_sizes=(0.1, 0.3),
-            min_vpa=1.0, max_vpa=1e4, weights=(4.0, 1.0)):
+            min_vpa=1.0, max_vpa=1e4, weights=(4.0, 1.0), d_min=None, d_min_types=False):
     """LJ NPT (or semi-grand with identity moves) case with P runs."""
     lj = create_lj(epsilon=epsilon, sigma=sigma, cutoff=cutoff, supercell_trafo=supercell)
     S = lj.n_species
@@ -48,7 +49,13 @@ def lj_case(P=1, K=32, N=8, seed=0, n_reflect=4, T=5, pressure=0.1, epsilon=1.0,
     elif identity == "both":
         moves.append(mvs.morph_move(S, weight=1.0))
         moves.append(mvs.swap_move(S, weight=1.0))
-    init_fn, step, _ = build_mwg(H, moves)
+    cons = ()
+    if d_min is not None:
+        from jaxrens_b200.constraints import min_distance_descriptor
+
+        dm = np.broadcast_to(np.asarray(d_min, np.float32), (S, S))
+        cons = (min_distance_descriptor(dm, type_dependent=d_min_types),)
+    init_fn, step, _ = build_mwg(H, moves, cons)
     root = prng.key(seed)
     keys = prng.split(root, P + 1)
     pos, cells, types = [], [], []

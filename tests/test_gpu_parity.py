@@ -207,6 +207,23 @@ def test_supercell_images_match_oracle():
     _compare(case, ns, infos, reps, hist)
 
 
+@pytest.mark.parametrize("types_dep", [False, True])
+def test_min_distance_gate_matches_oracle(types_dep):
+    """A minimum-distance constraint (constraints/min_distance.py) gates the
+    moves that can violate it; undone moves, reason-4 drops from the bucket
+    counts and all walker state identical to the oracle."""
+    dmin = [[0.6, 0.5], [0.5, 0.4]] if types_dep else 0.6
+    case = lj_case(P=2, K=16, N=6, seed=80 + int(types_dep), n_reflect=2, T=4,
+                   identity="morph", epsilon=[1.0, 0.5], sigma=[1.0, 0.9], d_min=dmin,
+                   d_min_types=types_dep, pressure=np.array([0.1, 0.3]))
+    ns, infos = _run_gpu(case, 12, 4)
+    reps, hist = _run_oracle(case, 12, 4)
+    _compare(case, ns, infos, reps, hist)
+    n_prop = sum(_np(i.n_proposed).sum() for i in infos)
+    n_rr = sum(_np(i.reject_reason_counts).sum() for i in infos)
+    assert n_rr < n_prop   # the gate undid some accepted moves
+
+
 @pytest.mark.parametrize("P,n_cull,n_extra", [(1, 3, 0), (1, 4, 2), (2, 2, 1)])
 def test_multi_cull_matches_oracle(P, n_cull, n_extra):
     """n_cull > 1 (nested_sampling.py:195-212): lexsort cull order, permuted

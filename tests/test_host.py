@@ -223,3 +223,50 @@ def test_oracle_multi_cull_invariants():
         assert rep.log_evidence[0] >= last
         last = rep.log_evidence[0]
         assert rep.energy.max() <= info.emax
+
+
+def test_min_distance_gates_the_moves_that_can_violate_it():
+    """make_move_gate (constraints/base.py:101-140): a uniform threshold gates
+    the position/cell moves only; a per-species one also the relabelling
+    moves.  A violating accepted move is undone with reason 4, which the
+    4-bucket reject counts drop (nested_sampling.py:562-570)."""
+    from tests._cases import lj_case, oracle_replicas
+
+    c = lj_case(P=1, K=16, N=6, seed=16, n_reflect=2, T=4, identity="morph",
+                epsilon=[1.0, 0.5], sigma=[1.0, 0.9], d_min=0.6)
+    assert [c["step"].params.moves.gate[m] for m in range(3)] == [1, 1, 0]
+    c2 = lj_case(P=1, K=16, N=6, seed=16, n_reflect=2, T=4, identity="morph",
+                 epsilon=[1.0, 0.5], sigma=[1.0, 0.9], d_min=[[0.6, 0.5], [0.5, 0.4]],
+                 d_min_types=True)
+    assert [c2["step"].params.moves.gate[m] for m in range(3)] == [1, 1, 1]
+    rep = oracle_replicas(c)[0]
+    dropped = 0
+    for _ in range(20):
+        info, *_ = O.ns_step(c["model"], c["moves"], rep, 4, prior_mass.log_alpha(16, 1),
+                             float(prior_mass.iteration_offsets(16, 1)[1][0]))
+        dropped += sum(info.n_prop[:3]) - sum(info.rr[:12])
+        for m in range(3):
+            assert info.rr[4 * m] == info.n_acc[m]
+    assert dropped > 0   # some moves met the gate
+
+
+def test_min_distance_predicate_matches_brute_force():
+    """The oracle gate's verdict equals a float64 brute-force minimum-image
+    distance check on random cubic configurations (away from the threshold)."""
+    rng = np.random.default_rng(5)
+    mv = O.make_moves([0], [1], [0.1], [1.0], gate=[1], dmin=[0.7])
+    hits = 0
+    for _ in range(40):
+        L = 2.5
+        x = rng.uniform(0, L, (6, 3)).astype(np.float32)
+        cell = (np.eye(3) * L).astype(np.float32)
+        d = x[:, None, :].astype(np.float64) - x[None, :, :]
+        d -= L * np.round(d / L)
+        r = np.sqrt((d ** 2).sum(-1))[np.triu_indices(6, 1)]
+        if np.any(np.abs(r - 0.7) < 1e-4):
+            continue
+        want = bool(np.all(r >= 0.7))
+        got = O.min_distance_ok(mv, 1, x, np.zeros(6, np.int32), cell)
+        assert got == want
+        hits += not want
+    assert hits > 0
