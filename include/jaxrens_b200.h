@@ -68,7 +68,7 @@ enum {
 
 enum { JR_MODEL_LJ = 0, JR_MODEL_GAUSS_MIX = 1 };
 enum { JR_MOVE_GALILEAN = 0, JR_MOVE_VOLUME = 1, JR_MOVE_MORPH = 2,
-       JR_MOVE_SWAP = 3 };
+       JR_MOVE_SWAP = 3, JR_MOVE_SHEAR = 4, JR_MOVE_STRETCH = 5 };
 
 typedef struct JrDims {
   int32_t n_replicas;      /* P */

@@ -17,7 +17,8 @@ from .backends import (
     create_lj,
     eval_energy_and_forces,
 )
-from .moves import MoveKernel, alchemical, galilean, gmc, morph_move, swap, swap_move, volume, volume_move
+from .moves import (MoveKernel, alchemical, galilean, gmc, morph_move, shear, shear_move, stretch,
+                    stretch_move, swap, swap_move, volume, volume_move)
 from .adaptation import adjust_step_size, build_adapt_step, process_rate
 from .burn_in import initial_walk, walk_population
 from .energy_log import EnergyLogCallback, EnergyLogger
@@ -40,7 +41,8 @@ from .nested_sampling import (
 __all__ = [
     "BackendResult", "EnsembleTerm", "GaussianMixtureBackend", "Hamiltonian", "LJBackend",
     "create_lj", "eval_energy_and_forces", "MoveKernel", "alchemical", "galilean", "gmc",
-    "morph_move", "swap", "swap_move", "volume", "volume_move", "build_mwg",
+    "morph_move", "swap", "swap_move", "volume", "volume_move", "shear", "shear_move",
+    "stretch", "stretch_move", "build_mwg",
     "InterREManager", "IterationTermination", "NSState", "PriorMassTermination",
     "final_log_evidence", "init_ns", "init_ns_parallel", "ns_iterate", "ns_step",
     "run_loop", "run_ns", "run_ns_parallel", "adjust_step_size", "build_adapt_step",

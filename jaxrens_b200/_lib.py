@@ -27,7 +27,7 @@ ERRORS = {
 }
 
 MODEL_LJ, MODEL_GAUSS_MIX = 0, 1
-MOVE_GALILEAN, MOVE_VOLUME, MOVE_MORPH, MOVE_SWAP = 0, 1, 2, 3
+MOVE_GALILEAN, MOVE_VOLUME, MOVE_MORPH, MOVE_SWAP, MOVE_SHEAR, MOVE_STRETCH = 0, 1, 2, 3, 4, 5
 
 _vp = C.c_void_p
 

@@ -965,7 +965,7 @@ int check_params(const JrDims* d, const JrParams* p) {
     return fail(JR_ERR_PARAM, "n_images must be in [1, 125]");
   for (int m = 0; m < d->n_moves; ++m) {
     const int t = p->moves.type[m];
-    if (t < 0 || t > JR_MOVE_SWAP) return fail(JR_ERR_PARAM, "unknown move type");
+    if (t < 0 || t > JR_MOVE_STRETCH) return fail(JR_ERR_PARAM, "unknown move type");
     if (t == JR_MOVE_GALILEAN && p->moves.n_reflect[m] < 1)
       return fail(JR_ERR_PARAM, "galilean n_reflect must be >= 1");
     if ((t == JR_MOVE_MORPH || t == JR_MOVE_SWAP) && p->model.n_species < 2)

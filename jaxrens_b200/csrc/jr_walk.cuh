@@ -941,6 +941,134 @@ __device__ __forceinline__ bool move_volume(const JrParams& P, Walker<G>& w, Key
   return acc;
 }
 
+// Cell-move tail shared by shear and stretch (moves/_common.py:16-93 without
+// a prior): positions x' = x . T (float32, the FMA order of the oracle), one
+// energy-only evaluation with the new cell, the cell-geometry guard; accept
+// iff the energy is under the contour and the cell is valid (energy > cell).
+template <class G>
+__device__ __forceinline__ bool move_cell(const JrParams& P, Walker<G>& w, const float* nc,
+                                          const float* T, double emax, float pressure,
+                                          const float* mu, int& reason) {
+  WalkShared& s = w.s;
+  const WalkArrays& arr = w.arr;
+  const int n = w.n;
+  const int r0 = w.g.rank(), gs = w.g.size();
+  const int cur = s.cur, tr = cur ^ 1;
+  for (int i = r0; i < n; i += gs) {
+    const float4 x = arr.xs[i];
+    arr.x0[3 * i] = x.x;
+    arr.x0[3 * i + 1] = x.y;
+    arr.x0[3 * i + 2] = x.z;
+    float y[3];
+    for (int q = 0; q < 3; ++q)
+      y[q] = __fmaf_rn(x.z, T[6 + q], __fmaf_rn(x.y, T[3 + q], __fmul_rn(x.x, T[q])));
+    arr.xs[i] = make_float4(y[0], y[1], y[2], x.w);
+  }
+  w.g.sync();
+  if (w.g.leader()) make_cell_ctx(nc, s.cc[tr], arr.T + tr * 3 * P.model.n_images, P.model);
+  w.g.sync();
+  double d0, d1;
+  const double En = ham_eval<false>(P, w, tr, pressure, mu, d0, d1);
+  const bool valid = cell_valid(nc, n, P.moves);
+  const bool energy_ok = En < emax;
+  const bool acc = energy_ok && valid;
+  reason = acc ? 0 : (!energy_ok ? 1 : 2);
+  if (!acc) {
+    for (int q = r0; q < 3 * n; q += gs) pos_at(arr.xs, q) = arr.x0[q];
+  }
+  w.g.sync();
+  if (w.g.leader() && acc) {
+    s.cur = tr;
+    s.E = En;
+  }
+  w.g.sync();
+  return acc;
+}
+
+// float32 norm of a 3-vector from a float64 sum of squares.
+__device__ __forceinline__ float norm3_f(const float* v) {
+  double q = __dadd_rn(0.0, __dmul_rn((double)v[0], (double)v[0]));
+  q = __dadd_rn(q, __dmul_rn((double)v[1], (double)v[1]));
+  q = __dadd_rn(q, __dmul_rn((double)v[2], (double)v[2]));
+  return __double2float_rn(__dsqrt_rn(q));
+}
+
+// shear (moves/shear.py:18-127): row a = randint(k1, 0, 3) moves by
+// rv1 v1n + rv2 v2n within the plane of the other two rows, (rv1, rv2) =
+// step * normal(k2, (2,)); T = solve(old, new) in float64.
+template <class G>
+__device__ __forceinline__ bool move_shear(const JrParams& P, Walker<G>& w, Key key, float step,
+                                           double emax, float pressure, const float* mu,
+                                           int& reason) {
+  const Key k1 = split(key, 0u), k2 = split(key, 1u);
+  const int a = randint(k1, 0, 3);
+  const float rv1 = __fmul_rn(step, normal(bits32(k2, 0u)));
+  const float rv2 = __fmul_rn(step, normal(bits32(k2, 1u)));
+  const float* h = w.s.cc[w.s.cur].raw;
+  const int b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;
+  const float* v1 = h + 3 * b;
+  const float* v2 = h + 3 * c;
+  float v1n[3], v2p[3], v2n[3];
+  const float n1 = norm3_f(v1);
+  for (int k = 0; k < 3; ++k) v1n[k] = __fdiv_rn(v1[k], n1);
+  double dd = __dadd_rn(0.0, __dmul_rn((double)v2[0], (double)v1n[0]));
+  dd = __dadd_rn(dd, __dmul_rn((double)v2[1], (double)v1n[1]));
+  dd = __dadd_rn(dd, __dmul_rn((double)v2[2], (double)v1n[2]));
+  const float dot = __double2float_rn(dd);
+  for (int k = 0; k < 3; ++k) v2p[k] = __fmaf_rn(-dot, v1n[k], v2[k]);
+  const float n2 = norm3_f(v2p);
+  for (int k = 0; k < 3; ++k) v2n[k] = __fdiv_rn(v2p[k], n2);
+  float nc[9];
+  for (int q = 0; q < 9; ++q) nc[q] = h[q];
+  for (int k = 0; k < 3; ++k)
+    nc[3 * a + k] = __fmaf_rn(rv2, v2n[k], __fmaf_rn(rv1, v1n[k], h[3 * a + k]));
+  double o[9], cof[9];
+  for (int q = 0; q < 9; ++q) o[q] = (double)h[q];
+  cof[0] = __dsub_rn(__dmul_rn(o[4], o[8]), __dmul_rn(o[5], o[7]));
+  cof[1] = __dsub_rn(__dmul_rn(o[5], o[6]), __dmul_rn(o[3], o[8]));
+  cof[2] = __dsub_rn(__dmul_rn(o[3], o[7]), __dmul_rn(o[4], o[6]));
+  cof[3] = __dsub_rn(__dmul_rn(o[2], o[7]), __dmul_rn(o[1], o[8]));
+  cof[4] = __dsub_rn(__dmul_rn(o[0], o[8]), __dmul_rn(o[2], o[6]));
+  cof[5] = __dsub_rn(__dmul_rn(o[1], o[6]), __dmul_rn(o[0], o[7]));
+  cof[6] = __dsub_rn(__dmul_rn(o[1], o[5]), __dmul_rn(o[2], o[4]));
+  cof[7] = __dsub_rn(__dmul_rn(o[2], o[3]), __dmul_rn(o[0], o[5]));
+  cof[8] = __dsub_rn(__dmul_rn(o[0], o[4]), __dmul_rn(o[1], o[3]));
+  const double det = __dadd_rn(__dadd_rn(__dmul_rn(o[0], cof[0]), __dmul_rn(o[1], cof[1])),
+                               __dmul_rn(o[2], cof[2]));
+  float T[9];
+  for (int k = 0; k < 3; ++k)
+    for (int q = 0; q < 3; ++q) {
+      double v = 0.0;
+      for (int m = 0; m < 3; ++m)
+        v = __dadd_rn(v, __dmul_rn(__ddiv_rn(cof[3 * m + k], det), (double)nc[3 * m + q]));
+      T[3 * k + q] = __double2float_rn(v);
+    }
+  return move_cell(P, w, nc, T, emax, pressure, mu, reason);
+}
+
+// stretch (moves/stretch.py:18-104): axes (i, j) = [(0,1), (0,2), (1,2)]
+// [randint(k1, 0, 3)], rv = step * normal(k2); T = diag with exp(rv) at i
+// and exp(-rv) at j (float64 exp rounded to float32); cell . T, x . T.
+template <class G>
+__device__ __forceinline__ bool move_stretch(const JrParams& P, Walker<G>& w, Key key,
+                                             float step, double emax, float pressure,
+                                             const float* mu, int& reason) {
+  const Key k1 = split(key, 0u), k2 = split(key, 1u);
+  const int pr = randint(k1, 0, 3);
+  const int ai = pr == 2 ? 1 : 0, aj = pr == 0 ? 1 : 2;
+  const float rv = __fmul_rn(step, normal(bits32(k2, 0u)));
+  float dg[3] = {1.0f, 1.0f, 1.0f};
+  dg[ai] = __double2float_rn(exp((double)rv));
+  dg[aj] = __double2float_rn(exp(-(double)rv));
+  const float* h = w.s.cc[w.s.cur].raw;
+  float T[9], nc[9];
+  for (int q = 0; q < 9; ++q) T[q] = 0.0f;
+  for (int k = 0; k < 3; ++k) T[4 * k] = dg[k];
+  for (int r = 0; r < 3; ++r)
+    for (int q = 0; q < 3; ++q) nc[3 * r + q] = __fmul_rn(h[3 * r + q], dg[q]);
+  return move_cell(P, w, nc, T, emax, pressure, mu, reason);
+}
+
 // alchemical_morph (alchemical.py:40-79).
 template <class G>
 __device__ __forceinline__ bool move_morph(const JrParams& P, Walker<G>& w, Key key, double emax,
@@ -1062,6 +1190,10 @@ __device__ __forceinline__ bool run_move(const JrParams& P, Walker<G>& w, int id
       reason = a ? 0 : 1;
       return a;
     }
+    case JR_MOVE_SHEAR:
+      return move_shear(P, w, key, step, emax, pressure, mu, reason);
+    case JR_MOVE_STRETCH:
+      return move_stretch(P, w, key, step, emax, pressure, mu, reason);
   }
   return false;
 }

@@ -88,7 +88,25 @@ def _swap_build_kernel(backend, n_species: int, species=None) -> MoveSpec:
     return MoveSpec(_lib.MOVE_SWAP)
 
 
+def _shear_build_kernel(backend, n_atoms: int, max_vol_per_atom: float = 100.0,
+                        min_vol_per_atom: float = 1.0, min_aspect: float = 0.5) -> MoveSpec:
+    """Volume-preserving shear of one cell vector (``shear.py:54-127``)."""
+    return MoveSpec(_lib.MOVE_SHEAR, cell_guard=(float(max_vol_per_atom),
+                                                 float(min_vol_per_atom), float(min_aspect),
+                                                 None))
+
+
+def _stretch_build_kernel(backend, n_atoms: int, max_vol_per_atom: float = 100.0,
+                          min_vol_per_atom: float = 1.0, min_aspect: float = 0.5) -> MoveSpec:
+    """Volume-preserving stretch along two axes (``stretch.py:18-104``)."""
+    return MoveSpec(_lib.MOVE_STRETCH, cell_guard=(float(max_vol_per_atom),
+                                                   float(min_vol_per_atom), float(min_aspect),
+                                                   None))
+
+
 galilean = SimpleNamespace(build_kernel=_galilean_build_kernel)
+shear = SimpleNamespace(build_kernel=_shear_build_kernel)
+stretch = SimpleNamespace(build_kernel=_stretch_build_kernel)
 volume = SimpleNamespace(build_kernel=_volume_build_kernel)
 alchemical = SimpleNamespace(build_morph_kernel=_morph_build_kernel)
 swap = SimpleNamespace(build_kernel=_swap_build_kernel)
@@ -132,3 +150,29 @@ def swap_move(n_species: int, weight: float = 1.0) -> MoveKernel:
     return MoveKernel("species_swap", swap.build_kernel,
                       kernel_kwargs={"n_species": n_species}, weight=weight,
                       step_size=0.0, mutates=frozenset({"types"}))
+
+
+def shear_move(n_atoms: int, step_size: float = 0.1, weight: float = 1.0,
+               max_volume_per_atom: float = 1e4, min_volume_per_atom: float = 1.0,
+               min_aspect_ratio: float = 0.8) -> MoveKernel:
+    """Convenience: ``moves[].type: shear`` with the ``cell:`` section defaults."""
+    return MoveKernel("shear", shear.build_kernel,
+                      kernel_kwargs={"n_atoms": n_atoms, "max_vol_per_atom": max_volume_per_atom,
+                                     "min_vol_per_atom": min_volume_per_atom,
+                                     "min_aspect": min_aspect_ratio},
+                      weight=weight, step_size=step_size,
+                      reject_reasons=frozenset({"energy", "cell"}),
+                      mutates=frozenset({"positions", "cell"}))
+
+
+def stretch_move(n_atoms: int, step_size: float = 0.1, weight: float = 1.0,
+                 max_volume_per_atom: float = 1e4, min_volume_per_atom: float = 1.0,
+                 min_aspect_ratio: float = 0.8) -> MoveKernel:
+    """Convenience: ``moves[].type: stretch`` with the ``cell:`` section defaults."""
+    return MoveKernel("stretch", stretch.build_kernel,
+                      kernel_kwargs={"n_atoms": n_atoms, "max_vol_per_atom": max_volume_per_atom,
+                                     "min_vol_per_atom": min_volume_per_atom,
+                                     "min_aspect": min_aspect_ratio},
+                      weight=weight, step_size=step_size,
+                      reject_reasons=frozenset({"energy", "cell"}),
+                      mutates=frozenset({"positions", "cell"}))

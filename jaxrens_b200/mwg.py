@@ -58,10 +58,14 @@ def _move_params(specs: list[MoveSpec], probs_cum: np.ndarray) -> _lib.JrMovePar
     if M > _lib.MAX_MOVES:
         raise ValueError("at most 8 move types")
     mv.n_moves = M
-    guards = {s.cell_guard for s in specs if s.cell_guard is not None}
+    # one cell-geometry guard for every cell move (the CLI's `cell:` section);
+    # the volume-prior flag comes from the volume move
+    guards = {s.cell_guard[:3] for s in specs if s.cell_guard is not None}
     if len(guards) > 1:
         raise NotImplementedError("all cell moves must share one cell-geometry guard")
-    max_vpa, min_vpa, min_aspect, flat = (guards.pop() if guards else (1e4, 1.0, 0.8, False))
+    max_vpa, min_vpa, min_aspect = guards.pop() if guards else (1e4, 1.0, 0.8)
+    flat = any(bool(s.cell_guard[3]) for s in specs
+               if s.cell_guard is not None and s.cell_guard[3] is not None)
     for m, s in enumerate(specs):
         mv.type[m] = s.type
         mv.n_reflect[m] = s.n_reflect

@@ -774,6 +774,109 @@ static int move_volume(const JroModel* mdl, const JroMoves* mv, int mode,
   return acc;
 }
 
+/* Cell move common tail (sampling/moves/_common.py:16-93 without a prior):
+ * positions x' = x . T, one energy, the cell-geometry guard, accept iff the
+ * energy is under the contour and the cell is valid (reason energy > cell). */
+static int cell_move_finish(const JroModel* mdl, const JroMoves* mv, int mode, double emax,
+                            int n, float* x, int32_t* t, float* cell, double* energy,
+                            float P, const float* mu, int has_mu, const float* nc,
+                            const float* T, int* reason) {
+  float* nx = (float*)malloc(sizeof(float) * 3 * n);
+  for (int i = 0; i < n; ++i)
+    for (int q = 0; q < 3; ++q) {
+      const float* xi = x + 3 * i;
+      nx[3 * i + q] = mode == JRO_REF32
+                          ? xi[0] * T[q] + xi[1] * T[3 + q] + xi[2] * T[6 + q]
+                          : fmaf(xi[2], T[6 + q], fmaf(xi[1], T[3 + q], xi[0] * T[q]));
+    }
+  double En = eval_energy(mdl, mode, n, nx, t, nc, P, mu, has_mu, NULL);
+  int valid = cell_valid(nc, n, mv->max_vpa, mv->min_vpa, mv->min_aspect, mode);
+  int energy_ok = En < emax;
+  int acc = energy_ok && valid;
+  *reason = acc ? 0 : (!energy_ok ? 1 : 2);
+  if (acc) {
+    memcpy(cell, nc, sizeof(float) * 9);
+    memcpy(x, nx, sizeof(float) * 3 * n);
+    *energy = En;
+  }
+  free(nx);
+  return acc;
+}
+
+/* shear (sampling/moves/shear.py:18-127): row a = randint(k1, 0, 3) moves by
+ * rv1 v1n + rv2 v2n in the plane of the other two rows (v1n the first of them
+ * normalised, v2n the second orthogonalised against it and normalised),
+ * (rv1, rv2) = step * normal(k2, (2,)); T = solve(old, new) in float64. */
+static int move_shear(const JroModel* mdl, const JroMoves* mv, int mode, const uint32_t key[2],
+                      float step, double emax, int n, float* x, int32_t* t, float* cell,
+                      double* energy, float P, const float* mu, int has_mu, int* reason) {
+  uint32_t k1[2], k2[2];
+  jro_split(key, 0, k1);
+  jro_split(key, 1, k2);
+  const int a = jro_randint(k1, 0, 3);
+  const float rv1 = step * jro_normal(jro_bits32(k2, 0));
+  const float rv2 = step * jro_normal(jro_bits32(k2, 1));
+  const int b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;
+  const float* v1 = cell + 3 * b;
+  const float* v2 = cell + 3 * c;
+  float v1n[3], v2p[3], v2n[3];
+  const float n1 = vnorm(v1, 3, mode);
+  for (int k = 0; k < 3; ++k) v1n[k] = v1[k] / n1;
+  float dot;
+  if (mode == JRO_REF32) {
+    dot = v2[0] * v1n[0] + v2[1] * v1n[1] + v2[2] * v1n[2];
+  } else {
+    double d = 0.0;
+    for (int k = 0; k < 3; ++k) d += (double)v2[k] * (double)v1n[k];
+    dot = (float)d;
+  }
+  for (int k = 0; k < 3; ++k)
+    v2p[k] = mode == JRO_REF32 ? v2[k] - dot * v1n[k] : fmaf(-dot, v1n[k], v2[k]);
+  const float n2 = vnorm(v2p, 3, mode);
+  for (int k = 0; k < 3; ++k) v2n[k] = v2p[k] / n2;
+  float nc[9];
+  memcpy(nc, cell, sizeof(nc));
+  for (int k = 0; k < 3; ++k)
+    nc[3 * a + k] = mode == JRO_REF32 ? cell[3 * a + k] + rv1 * v1n[k] + rv2 * v2n[k]
+                                      : fmaf(rv2, v2n[k], fmaf(rv1, v1n[k], cell[3 * a + k]));
+  double o[9], inv[9];
+  for (int q = 0; q < 9; ++q) o[q] = (double)cell[q];
+  inv_cell_f64(o, inv);
+  float T[9];
+  for (int k = 0; k < 3; ++k)
+    for (int q = 0; q < 3; ++q) {
+      double v = 0.0;
+      for (int m = 0; m < 3; ++m) v += inv[3 * k + m] * (double)nc[3 * m + q];
+      T[3 * k + q] = (float)v;
+    }
+  return cell_move_finish(mdl, mv, mode, emax, n, x, t, cell, energy, P, mu, has_mu, nc, T,
+                          reason);
+}
+
+/* stretch (sampling/moves/stretch.py:18-104): axes (i, j) = [(0,1), (0,2),
+ * (1,2)][randint(k1, 0, 3)], rv = step * normal(k2); T = diag with
+ * exp(rv) at i and exp(-rv) at j (float64 exp rounded to float32);
+ * new cell = cell . T, positions x . T. */
+static int move_stretch(const JroModel* mdl, const JroMoves* mv, int mode, const uint32_t key[2],
+                        float step, double emax, int n, float* x, int32_t* t, float* cell,
+                        double* energy, float P, const float* mu, int has_mu, int* reason) {
+  uint32_t k1[2], k2[2];
+  jro_split(key, 0, k1);
+  jro_split(key, 1, k2);
+  const int pr = jro_randint(k1, 0, 3);
+  const int ai = pr == 2 ? 1 : 0, aj = pr == 0 ? 1 : 2;
+  const float rv = step * jro_normal(jro_bits32(k2, 0));
+  float dg[3] = {1.0f, 1.0f, 1.0f};
+  dg[ai] = (float)exp((double)rv);
+  dg[aj] = (float)exp(-(double)rv);
+  float T[9] = {0}, nc[9];
+  for (int k = 0; k < 3; ++k) T[4 * k] = dg[k];
+  for (int r = 0; r < 3; ++r)
+    for (int q = 0; q < 3; ++q) nc[3 * r + q] = cell[3 * r + q] * dg[q];
+  return cell_move_finish(mdl, mv, mode, emax, n, x, t, cell, energy, P, mu, has_mu, nc, T,
+                          reason);
+}
+
 /* alchemical_morph (sampling/moves/alchemical.py:40-79). */
 static int move_morph(const JroModel* mdl, int mode, const uint32_t key[2],
                       double emax, int n, float* x, int32_t* t, float* cell,
@@ -931,6 +1034,14 @@ int32_t jro_move_trial(const JroModel* mdl, const JroMoves* mv, int32_t mode,
     case JRO_MOVE_SWAP:
       acc = move_swap(mdl, mode, key, emax, n, x, t, cell, energy, P, mu, has_mu);
       reason = acc ? 0 : 1;
+      break;
+    case JRO_MOVE_SHEAR:
+      acc = move_shear(mdl, mv, mode, key, step, emax, n, x, t, cell, energy, P, mu, has_mu,
+                       &reason);
+      break;
+    case JRO_MOVE_STRETCH:
+      acc = move_stretch(mdl, mv, mode, key, step, emax, n, x, t, cell, energy, P, mu, has_mu,
+                         &reason);
       break;
   }
   *energy = round_energy(*energy, mode);

@@ -37,7 +37,7 @@ extern "C" {
 
 enum { JRO_DEV = 0, JRO_REF32 = 1, JRO_F64 = 2 };
 enum { JRO_MOVE_GALILEAN = 0, JRO_MOVE_VOLUME = 1, JRO_MOVE_MORPH = 2,
-       JRO_MOVE_SWAP = 3 };
+       JRO_MOVE_SWAP = 3, JRO_MOVE_SHEAR = 4, JRO_MOVE_STRETCH = 5 };
 enum { JRO_MODEL_LJ = 0, JRO_MODEL_GAUSS_MIX = 1 };
 
 #define JRO_MAX_SPECIES 8

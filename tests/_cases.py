@@ -33,7 +33,8 @@ def oracle_moves(step) -> O.JroMoves:
 def lj_case(P=1, K=32, N=8, seed=0, n_reflect=4, T=5, pressure=0.1, epsilon=1.0,
             sigma=1.0, cutoff=2.5, supercell=(1, 1, 1), v_hi_per_atom=8.0,
             n_atoms_list=None, mu=None, identity=None, step_sizes=(0.1, 0.3),
-            min_vpa=1.0, max_vpa=1e4, weights=(4.0, 1.0), d_min=None, d_min_types=False):
+            min_vpa=1.0, max_vpa=1e4, weights=(4.0, 1.0), d_min=None, d_min_types=False,
+            cell_moves=False):
     """LJ NPT (or semi-grand with identity moves) case with P runs."""
     lj = create_lj(epsilon=epsilon, sigma=sigma, cutoff=cutoff, supercell_trafo=supercell)
     S = lj.n_species
@@ -42,6 +43,11 @@ def lj_case(P=1, K=32, N=8, seed=0, n_reflect=4, T=5, pressure=0.1, epsilon=1.0,
     moves = [mvs.gmc(n_reflect=n_reflect, step_size=step_sizes[0], weight=weights[0]),
              mvs.volume_move(max(Ns), step_size=step_sizes[1], weight=weights[1],
                              min_volume_per_atom=min_vpa, max_volume_per_atom=max_vpa)]
+    if cell_moves:
+        moves.append(mvs.shear_move(max(Ns), step_size=0.15, weight=1.0,
+                                    min_volume_per_atom=min_vpa, max_volume_per_atom=max_vpa))
+        moves.append(mvs.stretch_move(max(Ns), step_size=0.15, weight=1.0,
+                                      min_volume_per_atom=min_vpa, max_volume_per_atom=max_vpa))
     if identity == "morph":
         moves.append(mvs.morph_move(S, weight=1.0))
     elif identity == "swap":

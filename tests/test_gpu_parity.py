@@ -207,6 +207,22 @@ def test_supercell_images_match_oracle():
     _compare(case, ns, infos, reps, hist)
 
 
+def test_shear_and_stretch_moves_match_oracle():
+    """Shear (shear.py) and stretch (stretch.py) cell moves beside galilean and
+    volume: walkers, keys and counters identical to the oracle; the sheared
+    cells take the triclinic minimum-image path."""
+    case = lj_case(P=2, K=16, N=6, seed=90, n_reflect=2, T=6, cell_moves=True,
+                   pressure=np.array([0.1, 0.5]))
+    ns, infos = _run_gpu(case, 14, 6, chunk=5)
+    reps, hist = _run_oracle(case, 14, 6)
+    _compare(case, ns, infos, reps, hist)
+    cells = _np(ns.population.cell)
+    off = cells * (1 - np.eye(3, dtype=np.float32))
+    assert (np.abs(off) > 0).any()
+    acc = sum(_np(i.n_accepted).sum(axis=(0, 1)) for i in infos)
+    assert acc[2] > 0 and acc[3] > 0
+
+
 @pytest.mark.parametrize("types_dep", [False, True])
 def test_min_distance_gate_matches_oracle(types_dep):
     """A minimum-distance constraint (constraints/min_distance.py) gates the

@@ -270,3 +270,37 @@ def test_min_distance_predicate_matches_brute_force():
         assert got == want
         hits += not want
     assert hits > 0
+
+
+def test_oracle_shear_and_stretch_preserve_volume_and_fractions():
+    """shear.py / stretch.py: both proposals keep the cell volume (to float32
+    rounding) and map positions with the cell (fractional coordinates kept)."""
+    from jaxrens_b200 import moves as mv_
+    from tests._cases import lj_case, oracle_replicas
+
+    c = lj_case(P=1, K=8, N=5, seed=17, n_reflect=2, T=1, cell_moves=True)
+    assert [c["step"].params.moves.type[m] for m in range(4)] == [0, 1, 4, 5]
+    rep = oracle_replicas(c)[0]
+    for m in (2, 3):
+        n_acc = 0
+        for k in range(8):
+            for s in range(6):
+                key = prng.fold_in(prng.key(100 + s), k)
+                acc, x, d, t, cell, e, reason = O.move_trial(
+                    c["model"], c["moves"], m, key, 0.2, np.inf, rep.positions[k],
+                    rep.direction[k], rep.types[k], rep.cell[k], rep.energy[k],
+                    pressure=0.1)
+                if not acc:
+                    assert reason == 2   # infinite contour: only the cell guard rejects
+                    continue
+                n_acc += 1
+                v0 = abs(np.linalg.det(rep.cell[k].astype(np.float64)))
+                v1 = abs(np.linalg.det(cell.astype(np.float64)))
+                assert abs(v1 - v0) <= 1e-5 * v0
+                f0 = rep.positions[k].astype(np.float64) @ np.linalg.inv(rep.cell[k].astype(np.float64))
+                f1 = x.astype(np.float64) @ np.linalg.inv(cell.astype(np.float64))
+                assert np.abs(f1 - f0).max() < 1e-4
+        assert n_acc > 0
+    with pytest.raises(NotImplementedError):
+        build_mwg(create_lj(), [mv_.volume_move(4, min_aspect_ratio=0.8),
+                                mv_.shear_move(4, min_aspect_ratio=0.5)])
