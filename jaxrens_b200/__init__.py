@@ -23,6 +23,7 @@ from .adaptation import adjust_step_size, build_adapt_step, process_rate
 from .burn_in import initial_walk, walk_population
 from .energy_log import EnergyLogCallback, EnergyLogger
 from .mwg import build_mwg
+from . import thermo
 from .nested_sampling import (
     InterREManager,
     IterationTermination,

@@ -167,12 +167,12 @@ __device__ __forceinline__ double logaddexp(double a, double b) {
   return amax + log1p(exp(-fabs(delta)));
 }
 
-template <class G>
+template <bool kExt, class G>
 __device__ __forceinline__ void walk_chain(const JrParams& P, Walker<G>& w, int T, Key chain_key,
                                   Key move_key, double emax, float pressure, const float* mu) {
   for (int t = 0; t < T; ++t)
-    mwg_step(P, w, split(chain_key, (uint32_t)t), split(move_key, (uint32_t)t), emax, pressure,
-             mu);
+    mwg_step<kExt>(P, w, split(chain_key, (uint32_t)t), split(move_key, (uint32_t)t), emax,
+                   pressure, mu);
   w.g.sync();
 }
 
@@ -332,7 +332,7 @@ __device__ inline void build_group_pair_table(const G& g, uint16_t* pij, int n) 
   g.sync();
 }
 
-template <class G, int kMaxThreads>
+template <class G, int kMaxThreads, bool kExt>
 __global__ void __launch_bounds__(kMaxThreads, 1)
 ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
                   const JrInfoBuffers info, const int n_iter, const int tpa, const int C,
@@ -442,8 +442,8 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
         const int dst = is_clone ? (ncull > 1 ? ns.cw[sidx] : ns.worst[0]) : src;
         if (is_clone) write_dead(w.g, D, st, info, committed, p, dst, n, sidx);
         load_walker(P, D, st, w, p, src, is_clone);
-        walk_chain(P, w, T, split(ns.kmcmc[0], (uint32_t)sidx), ns.kmove[0], ns.e[0], pressure,
-                   mu);
+        walk_chain<kExt>(P, w, T, split(ns.kmcmc[0], (uint32_t)sidx), ns.kmove[0], ns.e[0],
+                         pressure, mu);
         store_walker(D, st, w, p, dst);
       }
     } else {
@@ -451,7 +451,8 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
       if (d < Dr && ns.spec[d]) {
         const int src = wi == 0 ? ns.clone[d] : ns.extras[d * nx + wi - 1];
         load_walker(P, D, st, w, p, src, wi == 0);
-        walk_chain(P, w, T, split(ns.kmcmc[d], (uint32_t)wi), ns.kmove[d], ns.e[d], pressure, mu);
+        walk_chain<kExt>(P, w, T, split(ns.kmcmc[d], (uint32_t)wi), ns.kmove[d], ns.e[d], pressure,
+                         mu);
         if (w.g.leader()) ns.res_E[my] = w.s.E;
       }
     }
@@ -607,7 +608,7 @@ move_trial_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st, co
     idx = choice(mk, P.moves.cum_probs, P.moves.n_moves);
   }
   int reason = 0;
-  const bool acc = gated_move(P, w, idx, key, step[p], emax[p], st.pressure[p], mu, reason);
+  const bool acc = gated_move<true>(P, w, idx, key, step[p], emax[p], st.pressure[p], mu, reason);
   w.g.sync();
   if (w.g.leader()) {
     accepted[tb] = acc ? 1 : 0;
@@ -662,7 +663,7 @@ walk_population_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers s
   const float* mu = st.mu ? st.mu + (size_t)p * P.model.n_species : nullptr;
   const Key rk{run_keys[2 * p], run_keys[2 * p + 1]};
   const Key mk{move_key[0], move_key[1]};
-  walk_chain(P, w, walklength, split(rk, (uint32_t)slot), mk, emax[p], st.pressure[p], mu);
+  walk_chain<true>(P, w, walklength, split(rk, (uint32_t)slot), mk, emax[p], st.pressure[p], mu);
   store_walker(D, st, w, p, slot);
 }
 
@@ -1005,17 +1006,24 @@ size_t group_dyn_smem(int nmax, int nimg, int groups) {
   return (size_t)groups * (jr::pair_table_bytes(nmax, nimg) + jr::walker_smem_bytes(nmax, nimg));
 }
 
-template <class G>
-int launch_ns(const JrDims* dims, const JrParams* params, const JrStateBuffers* state,
-              const JrInfoBuffers& inf, int n_iter, const JrLaunchConfig& c, void* workspace,
-              cudaStream_t s) {
+// Moves outside the lean walk: a constraint gate or a shear/stretch move.
+bool needs_ext_walk(const JrParams* p) {
+  for (int m = 0; m < p->moves.n_moves; ++m)
+    if (p->moves.gate[m] || p->moves.type[m] >= JR_MOVE_SHEAR) return true;
+  return false;
+}
+
+template <class G, bool kExt>
+int launch_ns_as(const JrDims* dims, const JrParams* params, const JrStateBuffers* state,
+                 const JrInfoBuffers& inf, int n_iter, const JrLaunchConfig& c, void* workspace,
+                 cudaStream_t s) {
+  constexpr int kT = std::is_same<G, jr::WarpGroup>::value ? 128 : 512;
+  auto kern = jr::ns_iterate_kernel<G, kT, kExt>;
   const size_t smem = ns_dyn_smem(dims, params, c);
-  cudaError_t e = cudaFuncSetAttribute(jr::ns_iterate_kernel<G, std::is_same<G, jr::WarpGroup>::value ? 128 : 512>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "smem attribute");
   if (c.cluster > 8) {
-    e = cudaFuncSetAttribute(jr::ns_iterate_kernel<G, std::is_same<G, jr::WarpGroup>::value ? 128 : 512>,
-                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e != cudaSuccess) return cuda_fail(e, "non-portable cluster attribute");
   }
   cudaLaunchConfig_t lc = {};
@@ -1030,10 +1038,19 @@ int launch_ns(const JrDims* dims, const JrParams* params, const JrStateBuffers* 
   attr[0].val.clusterDim.z = 1;
   lc.attrs = attr;
   lc.numAttrs = 1;
-  e = cudaLaunchKernelEx(&lc, jr::ns_iterate_kernel<G, std::is_same<G, jr::WarpGroup>::value ? 128 : 512>, *dims, *params, *state, inf, n_iter,
-                         (int)c.tpa, (int)c.cluster, (const uint32_t*)workspace);
+  e = cudaLaunchKernelEx(&lc, kern, *dims, *params, *state, inf, n_iter, (int)c.tpa,
+                         (int)c.cluster, (const uint32_t*)workspace);
   if (e != cudaSuccess) return cuda_fail(e, "ns_iterate launch");
   return JR_OK;
+}
+
+template <class G>
+int launch_ns(const JrDims* dims, const JrParams* params, const JrStateBuffers* state,
+              const JrInfoBuffers& inf, int n_iter, const JrLaunchConfig& c, void* workspace,
+              cudaStream_t s) {
+  if (needs_ext_walk(params))
+    return launch_ns_as<G, true>(dims, params, state, inf, n_iter, c, workspace, s);
+  return launch_ns_as<G, false>(dims, params, state, inf, n_iter, c, workspace, s);
 }
 
 }  // namespace

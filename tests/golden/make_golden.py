@@ -11,6 +11,10 @@ Writes
   lj8_energies.json header and first rows of lj8_npt.energies (format pin).
   prior_mass.json   outputs of the reference's numpy-only prior_mass.py
                     (log_alpha, iteration_offsets, log_dead_weights).
+  thermo.json       outputs of the reference's numpy/scipy-only
+                    postprocess/thermodynamics.py (log_evidence,
+                    partition_function, heat_capacity) on seeded synthetic
+                    dead/live energies.
 """
 
 from __future__ import annotations
@@ -64,6 +68,32 @@ def main(ref_root: str) -> None:
                       "log_live_weight_30": float(pm.log_live_weight(30, K, nc))})
     json.dump({"cases": cases, "source": "src/jaxrens/prior_mass.py"},
               open(os.path.join(HERE, "prior_mass.json"), "w"), indent=1)
+    # thermodynamics.py imports only jaxrens.prior_mass: serve the module
+    # loaded above under that name instead of importing the (JAX) package
+    import types
+
+    pkg = types.ModuleType("jaxrens")
+    pkg.__path__ = []
+    sys.modules.setdefault("jaxrens", pkg)
+    sys.modules["jaxrens.prior_mass"] = pm
+    spec = importlib.util.spec_from_file_location(
+        "ref_thermo", os.path.join(ref_root, "src/jaxrens/postprocess/thermodynamics.py"))
+    th = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(th)
+    rng = np.random.default_rng(2024)
+    tcases = []
+    for K, nc, n_dead in [(32, 1, 300), (64, 3, 450)]:
+        dead = np.sort(rng.normal(0.0, 3.0, n_dead))[::-1] + np.linspace(5.0, -5.0, n_dead)
+        live = dead[-1] - np.abs(rng.normal(0.0, 0.5, K))
+        betas = [0.2, 0.7, 1.0, 2.5]
+        tcases.append({
+            "n_live": K, "n_cull": nc, "dead": dead.tolist(), "live": live.tolist(),
+            "betas": betas,
+            "log_evidence": float(th.log_evidence(dead, live, K, nc)),
+            "partition_function": [float(th.partition_function(b, dead, live, K, nc)) for b in betas],
+            "heat_capacity": [float(th.heat_capacity(b, dead, live, K, nc)) for b in betas]})
+    json.dump({"cases": tcases, "source": "src/jaxrens/postprocess/thermodynamics.py"},
+              open(os.path.join(HERE, "thermo.json"), "w"), indent=1)
 
 
 if __name__ == "__main__":

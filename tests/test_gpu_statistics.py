@@ -1,0 +1,84 @@
+"""Statistical parity on the B200 (the north star's fourth check).
+
+* Gaussian-mixture toy (backends/toy.py:163-204): the evidence of GPU runs
+  matches the analytic log Z on its uniform prior cube.
+* LJ8 NPT: an ensemble of GPU runs and an ensemble of runs of the oracle in
+  the reference's float32 arithmetic (independent seeds) give the same log Z
+  and the same heat-capacity peak temperature within statistical error.
+"""
+
+import numpy as np
+import pytest
+
+from jaxrens_b200 import GaussianMixtureBackend, build_mwg, prior_mass, prng, thermo
+from jaxrens_b200 import moves as mvs
+from jaxrens_b200 import nested_sampling as nsm
+from oracle import oracle as O
+from tests._cases import lj_case, oracle_replicas
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _run_gpu(ns, step, n_iter, T, chunk=500):
+    dead = []
+    done = 0
+    while done < n_iter:
+        c = min(chunk, n_iter - done)
+        info = nsm.ns_iterate(ns, step, c, T)
+        dead.append(info.dead_energy.cpu().numpy())
+        done += c
+    torch.cuda.synchronize()
+    return np.concatenate(dead, axis=0).T, ns.population.energy64.cpu().numpy()
+
+
+def test_gaussian_mixture_log_evidence_is_analytic():
+    g = GaussianMixtureBackend(centers=[[-1.0, 0.0, 0.0], [1.0, 0.0, 0.0]], sigma=0.5)
+    h, K, P, T, n_iter = 3.0, 256, 4, 20, 2600
+    init_fn, step, _ = build_mwg(g, [mvs.gmc(n_reflect=4, step_size=0.1, weight=1.0)])
+    keys = prng.split(prng.key(31), P + 1)
+    pos = [prng.uniform(keys[r], K * 3).reshape(K, 1, 3) * np.float32(2 * h) - np.float32(h)
+           for r in range(P)]
+    ns = nsm.init_ns_parallel(init_fn, pos, [np.zeros((K, 1), np.int32)] * P, None,
+                              [np.zeros((K, 3, 3), np.float32)] * P,
+                              prng.split(keys[P], P))
+    dead, live = _run_gpu(ns, step, n_iter, T)
+    want = g.log_evidence(h)
+    lz = np.array([thermo.log_evidence(dead[r], live[r], K) for r in range(P)])
+    # the kernel's own accumulator plus the live share agrees with post-processing
+    np.testing.assert_allclose(nsm.final_log_evidence(ns).cpu().numpy(), lz, rtol=0, atol=1e-8)
+    assert np.all(np.abs(lz - want) < 0.5), (lz, want)
+    assert abs(lz.mean() - want) < 0.3, (lz, want)
+
+
+def _cv_peak(dead, live, K, n_atoms):
+    temps = np.linspace(0.05, 2.0, 196)
+    return thermo.cv_peak_temperature(temps, dead, live, K, 1, n_atoms)
+
+
+def test_lj8_npt_log_z_and_cv_peak_match_reference_arithmetic():
+    P, K, N, T, n_iter = 8, 64, 8, 8, 2000
+    la = prior_mass.log_alpha(K, 1)
+    wo = float(prior_mass.iteration_offsets(K, 1)[1][0])
+    gcase = lj_case(P=P, K=K, N=N, seed=100, n_reflect=4, T=T, pressure=0.1)
+    ns = nsm.init_ns_parallel(gcase["init_fn"], gcase["positions"], gcase["types"],
+                              gcase["energies"], gcase["cells"], gcase["run_keys"],
+                              ensemble_params={"pressure": gcase["pressures"]})
+    dead_g, live_g = _run_gpu(ns, gcase["step"], n_iter, T)
+    rcase = lj_case(P=P, K=K, N=N, seed=200, n_reflect=4, T=T, pressure=0.1)
+    reps = oracle_replicas(rcase)
+    dead_r = np.zeros((P, n_iter))
+    for it in range(n_iter):
+        infos = O.ns_step_batched(rcase["model"], rcase["moves"], reps, T, la, wo,
+                                  shared_move_key=True, mode=O.REF32, n_threads=8)
+        dead_r[:, it] = [i.dead_energy for i in infos]
+    live_r = np.stack([r.energy for r in reps])
+    lz_g = np.array([thermo.log_evidence(dead_g[r], live_g[r], K) for r in range(P)])
+    lz_r = np.array([thermo.log_evidence(dead_r[r], live_r[r], K) for r in range(P)])
+    se = np.sqrt(lz_g.var(ddof=1) / P + lz_r.var(ddof=1) / P)
+    assert abs(lz_g.mean() - lz_r.mean()) < 4 * se + 0.05, (lz_g, lz_r)
+    tg = np.array([_cv_peak(dead_g[r], live_g[r], K, N) for r in range(P)])
+    tr = np.array([_cv_peak(dead_r[r], live_r[r], K, N) for r in range(P)])
+    se_t = np.sqrt(tg.var(ddof=1) / P + tr.var(ddof=1) / P)
+    assert abs(tg.mean() - tr.mean()) < 4 * se_t + 0.03, (tg, tr)

@@ -209,3 +209,17 @@ def test_energies_file_format_pin():
     assert (int(n_walkers), int(n_cull), int(n_atoms)) == (32, 1, 8)
     it, H, V = g["rows"][0].split()
     assert int(it) == 0 and float(H) > 0 and float(V) > 0
+
+
+def test_thermodynamics_match_reference_outputs():
+    """postprocess/thermodynamics.py restated: log Z, log Z(beta) and C_v on
+    the seeded fixture equal the reference module's own outputs."""
+    from jaxrens_b200 import thermo
+
+    g = json.load(open(os.path.join(GOLD, "thermo.json")))
+    for c in g["cases"]:
+        d, l, K, nc = np.array(c["dead"]), np.array(c["live"]), c["n_live"], c["n_cull"]
+        assert abs(thermo.log_evidence(d, l, K, nc) - c["log_evidence"]) <= 1e-12 * abs(c["log_evidence"])
+        for b, z, cv in zip(c["betas"], c["partition_function"], c["heat_capacity"]):
+            assert abs(thermo.partition_function(b, d, l, K, nc) - z) <= 1e-12 * max(1, abs(z))
+            assert abs(thermo.heat_capacity(b, d, l, K, nc) - cv) <= 1e-10 * max(1, abs(cv))
