@@ -2,7 +2,8 @@
  * jaxrens_b200.h -- C-ABI of the B200 nested-sampling walk.
  *
  * Drop-in boundary for jaxrens's jitted NS iteration.  Every buffer is a
- * device pointer owned by the caller (XLA, torch, or plain CUDA); the library
+ * device pointer owned by the caller (XLA, torch, or plain CUDA); apart from
+ * jr_autotune, which clones the state to time launch shapes on, the library
  * allocates nothing on the call path.  All entry points are asynchronous on
  * the given stream and return 0 on success or a negative JR_ERR_* code, with
  * a message available from jr_last_error().

@@ -47,6 +47,8 @@ struct NsShared {
   int extras[kMaxWalk];
   int wset[kMaxWalk];
   int n_wset;
+  Key kchain[kMaxD];        // fast predictions: run key of iteration d
+  Key k0chain[kMaxD];       // fast predictions: replica-0 key of iteration d
   int cw[JR_MAX_CULL];     // n_cull > 1: culled walkers, descending energy
   int cc[JR_MAX_CULL];     // n_cull > 1: their clone sources
   double ce[JR_MAX_CULL];  // n_cull > 1: culled energies
@@ -245,6 +247,106 @@ __device__ inline DynLayout dyn_layout(unsigned char* dyn, int K, int nmax, int 
   return L;
 }
 
+// The Dr predictions of a round for n_cull = 1 without extras and K <= 1024,
+// identical to Dr sequential cull_select/randint passes but without their
+// block barriers: warp 0 walks the run-key chain while warp 1 walks the
+// replica-0 key chain, lane d then derives iteration d's keys and raw clone
+// draw, and warp 0 selects the Dr culls from registers (walker k in lane
+// k % 32, bit k / 32 of a per-lane mask once culled): the maximum energy
+// (any NaN poisons it, culling walker 0), exact ties broken by the largest
+// uniform noise of that iteration's worst key, then the lowest index.
+__device__ void predict_fast(NsShared& ns, const double* E, int K, int Dr, Key key, Key key0,
+                             bool shared_mk) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (warp == 0) {
+    Key kd = key;
+    for (int d = 0; d < Dr; ++d) {
+      if (lane == 0) ns.kchain[d] = kd;
+      kd = split(split(kd, 0u), 0u);
+    }
+  } else if (warp == 1 && shared_mk) {
+    Key k0 = key0;
+    for (int d = 0; d < Dr; ++d) {
+      if (lane == 0) ns.k0chain[d] = k0;
+      k0 = advance_iteration(k0);
+    }
+  }
+  __syncthreads();
+  if (warp != 0) return;
+  // per-iteration keys and raw clone draws, one lane per iteration
+  Key my_kw{0u, 0u};
+  int my_raw = 0;
+  if (lane < Dr) {
+    const Key kd = ns.kchain[lane];
+    const Key ka = split(kd, 0u);
+    my_kw = split(kd, 1u);
+    my_raw = randint(split(ka, 1u), 0, K - 1);
+    ns.kmcmc[lane] = split(ka, 3u);
+    ns.kmove[lane] = shared_mk ? split(ns.k0chain[lane], 1u) : split(ka, 4u);
+  }
+  const int nslot = (K + 31) >> 5;
+  uint32_t taken = 0;
+  bool prev_ok = true;
+  double prev_e = 0.0;
+  for (int d = 0; d < Dr; ++d) {
+    unsigned long long best = 0;
+    int nanf = 0;
+    for (int j = 0; j < nslot; ++j) {
+      const int k = lane + 32 * j;
+      if (k >= K || ((taken >> j) & 1u)) continue;
+      const double x = E[k];
+      if (isnan(x)) {
+        nanf = 1;
+      } else {
+        const unsigned long long o = ord_double(x);
+        best = o > best ? o : best;
+      }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      const unsigned long long o = __shfl_xor_sync(0xffffffffu, best, off);
+      best = o > best ? o : best;
+      nanf |= __shfl_xor_sync(0xffffffffu, nanf, off);
+    }
+    const bool any_nan = nanf != 0;
+    int worst = 0;
+    double emax = __longlong_as_double(0x7ff8000000000000ll);
+    if (!any_nan) {
+      emax = unord_double(best);
+      const Key kw{__shfl_sync(0xffffffffu, my_kw.k0, d), __shfl_sync(0xffffffffu, my_kw.k1, d)};
+      unsigned long long tb = 0;
+      for (int j = 0; j < nslot; ++j) {
+        const int k = lane + 32 * j;
+        if (k >= K || ((taken >> j) & 1u) || E[k] != emax) continue;
+        const float nz = uniform01(bits32(kw, (uint32_t)k));
+        const unsigned long long t =
+            ((unsigned long long)__float_as_uint(nz) << 32) | (0xFFFFFFFFu - (unsigned)k);
+        tb = t > tb ? t : tb;
+      }
+      for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long o = __shfl_xor_sync(0xffffffffu, tb, off);
+        tb = o > tb ? o : tb;
+      }
+      worst = (int)(0xFFFFFFFFu - (unsigned)(tb & 0xFFFFFFFFull));
+    }
+    int clone = __shfl_sync(0xffffffffu, my_raw, d);
+    if (clone >= worst) clone += 1;
+    // a clone source culled earlier in the round breaks the prediction chain
+    const unsigned cbit = __shfl_sync(0xffffffffu, taken, clone & 31);
+    const bool conflict = d > 0 && ((cbit >> (clone >> 5)) & 1u);
+    const bool sp = d == 0 || (prev_ok && !any_nan && !isnan(prev_e) && !conflict);
+    if (lane == (worst & 31)) taken |= 1u << (worst >> 5);
+    if (lane == 0) {
+      ns.spec[d] = sp ? 1 : 0;
+      ns.worst[d] = worst;
+      ns.clone[d] = clone;
+      ns.e[d] = emax;
+      ns.wset[ns.n_wset++] = worst;
+    }
+    prev_ok = sp;
+    prev_e = emax;
+  }
+}
+
 // _select_culls for n_cull > 1 (nested_sampling.py:195-212).  order = the
 // walkers by descending energy (NaN last, as XLA's float sort places it),
 // then descending uniform noise, then index (lexsort((-noise, -E)));
@@ -380,8 +482,11 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
     if (threadIdx.x == 0) ns.n_wset = 0;
     __syncthreads();
     // ---- predictions for iterations d < Dr (every CTA, identically) ----
+    const bool fast = ncull == 1 && nx == 0 && K <= 1024 && blockDim.x >= 64;
+    if (fast) predict_fast(ns, L.Epop, K, Dr, key, key0, D.shared_move_key != 0);
+    __syncthreads();
     Key kd = key, k0d = key0;
-    for (int d = 0; d < Dr; ++d) {
+    for (int d = 0; d < (fast ? 0 : Dr); ++d) {
       const Key ka = split(kd, 0u), kw = split(kd, 1u);
       const Key kclone = split(ka, 1u), kextra = split(ka, 2u);
       const Key kmcmc = split(ka, 3u), kmoves = split(ka, 4u);
