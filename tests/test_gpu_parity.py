@@ -76,6 +76,31 @@ def test_energy_forces_bitwise_vs_oracle(kind):
         assert np.abs(F[b] - f64).max() <= 1e-5 * max(1.0, np.abs(f64).max())
 
 
+@pytest.mark.parametrize("N", [80, 100])
+def test_energy_forces_large_walkers_bitwise_vs_oracle(N):
+    """Walkers above 64 atoms: the pair-matrix path up to 96, the ordered
+    pairs beyond, both bit-exact against the oracle."""
+    rng = np.random.default_rng(N)
+    lj = create_lj(epsilon=1.0, sigma=1.0, cutoff=2.5)
+    H = Hamiltonian(lj, [EnsembleTerm(pressure=0.2)])
+    L = 1.25 * N ** (1.0 / 3.0)
+    pos, cell, types = _configs(rng, 6, N, L, triclinic=True)
+    res = H.energy_and_forces(pos, types, cell)
+    E, F = _np(res.energy), _np(res.forces)
+    m = oracle_model(H)
+    for b in range(6):
+        e_o, f_o, _ = O.energy(m, pos[b], types[b], cell[b], pressure=0.2, mode=O.DEV)
+        assert abs(E[b] - e_o) <= 1e-12 * max(1.0, abs(e_o)), (b, E[b], e_o)
+        np.testing.assert_array_equal(F[b], f_o.astype(np.float32))
+
+
+def test_large_walker_ns_run_matches_oracle():
+    case = lj_case(P=1, K=12, N=80, seed=8, n_reflect=2, T=2, v_hi_per_atom=3.0)
+    ns, infos = _run_gpu(case, 4, 2)
+    reps, hist = _run_oracle(case, 4, 2)
+    _compare(case, ns, infos, reps, hist)
+
+
 def test_gauss_mix_energy_vs_oracle():
     g = GaussianMixtureBackend(centers=[[-1, 0, 0], [1, 0.5, 0]], sigma=0.5)
     rng = np.random.default_rng(3)
