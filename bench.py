@@ -302,14 +302,36 @@ def run_ours(args):
 
 
 def end_to_end(args, ns, step, re, cfg, torch, nsm):
-    """Each step: pinned-host state -> device, 10 iterations + swap through
-    the public API, per-iteration results (dead energies, log Z) -> host."""
+    """Each step: the pinned-host state -> device (one copy), 10 iterations +
+    swap through the public API, per-iteration results (dead energies, log Z)
+    -> host."""
+    import dataclasses
+
     pop = ns.population
-    fields = [pop.positions, pop.direction, pop.types, pop.energy, pop.energy64, pop.cell,
-              pop.step_sizes, pop.n_accepted, pop.n_proposed, ns.rng_key, ns.log_evidence,
-              ns.iteration, ns.emax]
-    host = [f.detach().cpu().pin_memory() for f in fields]
-    h2d = sum(h.numel() * h.element_size() for h in host)
+    names_p = ["positions", "direction", "types", "energy", "energy64", "cell", "step_sizes",
+               "n_accepted", "n_proposed"]
+    names_s = ["rng_key", "log_evidence", "iteration", "emax"]
+    fields = [getattr(pop, k) for k in names_p] + [getattr(ns, k) for k in names_s]
+    # the whole state in one pinned host buffer and one device buffer (fields
+    # 256-byte aligned), so each step uploads it with a single copy; the
+    # state the API works on is views into the device buffer
+    offs, off = [], 0
+    for f in fields:
+        off = (off + 255) // 256 * 256
+        offs.append(off)
+        off += f.numel() * f.element_size()
+    flat_dev = torch.empty(off, dtype=torch.uint8, device=pop.positions.device)
+    flat_host = torch.zeros(off, dtype=torch.uint8).pin_memory()
+    views = []
+    for f, o in zip(fields, offs):
+        nb = f.numel() * f.element_size()
+        v = flat_dev[o:o + nb].view(f.dtype).view(f.shape)
+        v.copy_(f)
+        flat_host[o:o + nb].copy_(f.detach().contiguous().view(-1).view(torch.uint8).cpu())
+        views.append(v)
+    pop2 = dataclasses.replace(pop, **dict(zip(names_p, views[:len(names_p)])))
+    ns = dataclasses.replace(ns, population=pop2, **dict(zip(names_s, views[len(names_p):])))
+    h2d = off
     info = nsm.InfoBuffers(ns, step.n_moves, RE_INTERVAL, dead=False)
     out_e = torch.empty((RE_INTERVAL, P_RUNS), dtype=torch.float64).pin_memory()
     out_z = torch.empty((RE_INTERVAL, P_RUNS), dtype=torch.float64).pin_memory()
@@ -320,8 +342,7 @@ def end_to_end(args, ns, step, re, cfg, torch, nsm):
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record()
     for _ in range(n):
-        for f, h in zip(fields, host):
-            f.copy_(h, non_blocking=True)
+        flat_dev.copy_(flat_host, non_blocking=True)
         nsm.ns_iterate(ns, step, RE_INTERVAL, T, 0, info=info, cfg=cfg)
         re.apply(ns, step)
         out_e.copy_(info.emax, non_blocking=True)
