@@ -224,6 +224,20 @@ def test_uneven_semigrand_identity_moves_match_oracle():
     _compare(case, ns, infos, reps, hist)
 
 
+def test_uneven_semigrand_up_to_96_atoms_matches_oracle():
+    """The uneven semi-grand shape of the batched binary configuration: runs of
+    16, 56 and 96 atoms in one launch (Nmax 96, pair-matrix path with a
+    per-run row stride), Kob-Andersen pair tables, Delta-mu, morph and swap
+    identity moves."""
+    lj_pair = dict(epsilon=[[1.0, 1.5], [1.5, 0.5]], sigma=[[1.0, 0.8], [0.8, 0.88]])
+    case = lj_case(P=3, K=12, N=16, seed=9, n_reflect=2, T=3, n_atoms_list=[16, 56, 96],
+                   identity="both", mu=np.array([[0.0, -2.0], [0.0, 0.3], [0.0, 2.0]]),
+                   v_hi_per_atom=4.0, **lj_pair)
+    ns, infos = _run_gpu(case, 6, 3)
+    reps, hist = _run_oracle(case, 6, 3)
+    _compare(case, ns, infos, reps, hist)
+
+
 def test_supercell_images_match_oracle():
     case = lj_case(P=1, K=16, N=6, seed=5, n_reflect=3, T=3, supercell=(2, 2, 2),
                    v_hi_per_atom=6.0)
