@@ -573,6 +573,15 @@ __device__ __forceinline__ void pairs_matrix(const JrParams& P, Walker<G>& w, co
   const int apb = gs / L;
   const int blk = tid & (L - 1);
   double ff_part = 0.0, fd_part = 0.0;
+  // The energy partials are first summed over the L lanes of an atom group
+  // (every lane of the group ends with the group sum), so the group
+  // reduction below starts at stride L, where ff and fd live.  Warps that
+  // gather do it while their row loads are in flight.
+  bool ep_folded = false;
+  auto fold_ep = [&]() {
+    for (int off = 1; off < L; off <<= 1) ep += __shfl_xor_sync(0xffffffffu, ep, off);
+    ep_folded = true;
+  };
   for (int base = 0; base < n; base += apb) {
     const int i = base + tid / L;
     // warps whose atoms all lie beyond n leave the issue slots to the others
@@ -584,6 +593,7 @@ __device__ __forceinline__ void pairs_matrix(const JrParams& P, Walker<G>& w, co
     const int j0 = blk * 8;
     const int ic = i < n ? i : 0;
     const float* row = arr.pm + ic * S;
+    const float d0 = arr.dir[3 * ic], d1 = arr.dir[3 * ic + 1], d2 = arr.dir[3 * ic + 2];
     float vx[8], vy[8], vz[8];
 #pragma unroll
     for (int jj = 0; jj < 8; ++jj) {
@@ -595,6 +605,7 @@ __device__ __forceinline__ void pairs_matrix(const JrParams& P, Walker<G>& w, co
       vy[jj] = ok ? y : 0.0f;
       vz[jj] = ok ? z : 0.0f;
     }
+    if (!ep_folded) fold_ep();
 #pragma unroll
     for (int jj = 0; jj < 8; ++jj) {
       fx = __fadd_rn(fx, vx[jj]);
@@ -608,13 +619,12 @@ __device__ __forceinline__ void pairs_matrix(const JrParams& P, Walker<G>& w, co
       arr.F[3 * i + 2] = fz;
       const double dx = fx, dy = fy, dz = fz;
       ff_part = __fma_rn(dx, dx, __fma_rn(dy, dy, __fma_rn(dz, dz, ff_part)));
-      fd_part = __fma_rn(dx, (double)arr.dir[3 * i],
-                         __fma_rn(dy, (double)arr.dir[3 * i + 1],
-                                  __fma_rn(dz, (double)arr.dir[3 * i + 2], fd_part)));
+      fd_part = __fma_rn(dx, (double)d0, __fma_rn(dy, (double)d1, __fma_rn(dz, (double)d2, fd_part)));
     }
   }
+  if (!ep_folded) fold_ep();
   double e_part = ep;
-  w.g.sum3(e_part, ff_part, fd_part, 1, w.par);
+  w.g.sum3(e_part, ff_part, fd_part, L, w.par);
   U = e_part;
   sff = ff_part;
   sfd = fd_part;
@@ -780,6 +790,53 @@ __device__ __forceinline__ double group_sum1(Walker<G>& w, double v) {
 
 // ---------------------------------------------------------------- moves --
 
+// The R position updates and evaluations of one galilean trajectory.  The
+// pair path, the species branch and the cell geometry are chosen once for
+// the trajectory (the cell is fixed during the move), so each evaluation
+// starts directly on the pair loop; ens is the fixed P V - mu N share.
+// Returns the final potential (NaN read as +inf); the direction is reflected
+// off the contour in place.
+constexpr int kTrajModel = 0, kTrajMatrix = 1, kTrajOrdered = 2;
+
+template <int kPath, bool kS1, bool kDiag, class G>
+__device__ __forceinline__ double galilean_trajectory(const JrParams& P, Walker<G>& w, float step,
+                                                      int R, double emax, double ens) {
+  const WalkArrays& arr = w.arr;
+  const int n3 = 3 * w.n;
+  const int r0 = w.g.rank(), gs = w.g.size();
+  const int cidx = w.s.cur;
+  MicRegs cc;
+  if (kPath != kTrajModel) cc = load_mic<kDiag>(w.s.cc[cidx]);
+  const float* T = arr.T + cidx * 3 * P.model.n_images;
+  double E = w.s.E;
+  for (int r = 0; r < R; ++r) {
+    for (int q = r0; q < n3; q += gs) {
+      float& x = pos_at(arr.xs, q);
+      x = __fmaf_rn(step, arr.dir[q], x);
+    }
+    w.g.sync();
+    double U, sff, sfd;
+    if (kPath == kTrajMatrix) {
+      pairs_matrix<true, kS1, kDiag>(P, w, cc, U, sff, sfd);
+      E = U + ens;
+    } else if (kPath == kTrajOrdered) {
+      pairs_ordered<true, kS1, kDiag>(P, w, cc, T, U, sff, sfd);
+      E = U + ens;
+    } else {
+      model_eval<true>(P, w, cidx, U, sff, sfd);
+      E = U;
+    }
+    if (isnan(E)) E = INFINITY;
+    if (E >= emax) {
+      // d <- d - [2 (F.d) / max(|F|^2, 1e-20)] F, the scalar in float32
+      const float ffs = __double2float_rn(sff);
+      const float coef = __fmul_rn(2.0f * __double2float_rn(sfd), rcp_nr(ffs > 1e-20f ? ffs : 1e-20f));
+      for (int q = r0; q < n3; q += gs) arr.dir[q] = __fmaf_rn(-coef, arr.F[q], arr.dir[q]);
+    }
+  }
+  return E;
+}
+
 // Galilean move (galilean.py:142-300) with forces-based reflection.  The
 // reflection d - 2 (f.d) f with f = F/|F| is evaluated as
 // d - [2 (F.d) / max(|F|,1e-10)^2] F from two float64 sums.
@@ -790,22 +847,28 @@ __device__ __forceinline__ bool move_galilean(const JrParams& P, Walker<G>& w, K
   const int n3 = 3 * w.n;
   const int r0 = w.g.rank(), gs = w.g.size();
   const Key ki = split(key, 0u), kp = split(key, 1u);
-  double sq = 0.0;
-  for (int q = r0; q < n3; q += gs) sq += (double)arr.dir[q] * (double)arr.dir[q];
-  sq = group_sum1(w, sq);
-  const bool fresh = __double2float_rn(sqrt(sq)) < 1e-8f;
-  double sv = 0.0;
+  // |d|^2 and |d + pa * normal|^2 in one group reduction; a direction of
+  // norm < 1e-8 (a walker's first galilean move) then redraws a fresh normal
+  // direction and reduces its norm separately.  The sums are the ones of
+  // the two-pass form (same partials, same tree).
+  double sq = 0.0, sv = 0.0, zero = 0.0;
   for (int q = r0; q < n3; q += gs) {
-    float v;
-    if (fresh) {
-      v = normal(bits32(ki, (uint32_t)q));
-    } else {
-      v = __fmaf_rn(pa, normal(bits32(kp, (uint32_t)q)), arr.dir[q]);
-    }
-    arr.dir[q] = v;
+    const float d = arr.dir[q];
+    const float v = __fmaf_rn(pa, normal(bits32(kp, (uint32_t)q)), d);
+    sq += (double)d * (double)d;
     sv += (double)v * (double)v;
+    arr.dir[q] = v;
   }
-  sv = group_sum1(w, sv);
+  w.g.sum3(sq, sv, zero, 1, w.par);
+  if (__double2float_rn(sqrt(sq)) < 1e-8f) {
+    sv = 0.0;
+    for (int q = r0; q < n3; q += gs) {
+      const float v = normal(bits32(ki, (uint32_t)q));
+      arr.dir[q] = v;
+      sv += (double)v * (double)v;
+    }
+    sv = group_sum1(w, sv);
+  }
   const float nv = __double2float_rn(sqrt(sv));
   const float den = nv > 1e-10f ? nv : 1e-10f;
   for (int q = r0; q < n3; q += gs) {
@@ -815,21 +878,25 @@ __device__ __forceinline__ bool move_galilean(const JrParams& P, Walker<G>& w, K
     arr.x0[q] = pos_at(arr.xs, q);
   }
   const double E0 = w.s.E;
-  double E = E0;
-  for (int r = 0; r < R; ++r) {
-    for (int q = r0; q < n3; q += gs) {
-      float& x = pos_at(arr.xs, q);
-      x = __fmaf_rn(step, arr.dir[q], x);
-    }
-    w.g.sync();
-    double sff, sfd;
-    E = ham_eval<true>(P, w, w.s.cur, pressure, mu, sff, sfd);
-    if (isnan(E)) E = INFINITY;
-    if (E >= emax) {
-      // d <- d - [2 (F.d) / max(|F|^2, 1e-20)] F, the scalar in float32
-      const float ffs = __double2float_rn(sff);
-      const float coef = __fmul_rn(2.0f * __double2float_rn(sfd), rcp_nr(ffs > 1e-20f ? ffs : 1e-20f));
-      for (int q = r0; q < n3; q += gs) arr.dir[q] = __fmaf_rn(-coef, arr.F[q], arr.dir[q]);
+  double E;
+  const JrModelParams& mp = P.model;
+  if (mp.model == JR_MODEL_GAUSS_MIX) {
+    E = galilean_trajectory<kTrajModel, true, true>(P, w, step, R, emax, 0.0);
+  } else {
+    // the cell, the species counts and so P V - mu N are fixed for the move
+    const double ens = ensemble_term(w.s, w.s.cc[w.s.cur].vol, pressure, mu, mp.n_species);
+    const bool s1 = mp.n_species == 1;
+    const bool diag = w.s.cc[w.s.cur].diag != 0;
+    if (arr.pm != nullptr && mp.n_images == 1 && w.n <= kPairMatMax) {
+      if (diag) E = s1 ? galilean_trajectory<kTrajMatrix, true, true>(P, w, step, R, emax, ens)
+                       : galilean_trajectory<kTrajMatrix, false, true>(P, w, step, R, emax, ens);
+      else E = s1 ? galilean_trajectory<kTrajMatrix, true, false>(P, w, step, R, emax, ens)
+                  : galilean_trajectory<kTrajMatrix, false, false>(P, w, step, R, emax, ens);
+    } else {
+      if (diag) E = s1 ? galilean_trajectory<kTrajOrdered, true, true>(P, w, step, R, emax, ens)
+                       : galilean_trajectory<kTrajOrdered, false, true>(P, w, step, R, emax, ens);
+      else E = s1 ? galilean_trajectory<kTrajOrdered, true, false>(P, w, step, R, emax, ens)
+                  : galilean_trajectory<kTrajOrdered, false, false>(P, w, step, R, emax, ens);
     }
   }
   const bool acc = E < emax;
