@@ -169,13 +169,25 @@ __device__ __forceinline__ double logaddexp(double a, double b) {
   return amax + log1p(exp(-fabs(delta)));
 }
 
+// T MWG steps of one chain.  The step keys split(chain_key, t) and the move
+// choices (from split(move_key, t)) do not depend on the walk, so each chunk
+// of kStepChunk steps draws them up front, one step per thread.
 template <bool kExt, class G>
 __device__ __forceinline__ void walk_chain(const JrParams& P, Walker<G>& w, int T, Key chain_key,
                                   Key move_key, double emax, float pressure, const float* mu) {
-  for (int t = 0; t < T; ++t)
-    mwg_step<kExt>(P, w, split(chain_key, (uint32_t)t), split(move_key, (uint32_t)t), emax,
-                   pressure, mu);
-  w.g.sync();
+  WalkShared& s = w.s;
+  for (int t0 = 0; t0 < T; t0 += kStepChunk) {
+    const int nt = T - t0 < kStepChunk ? T - t0 : kStepChunk;
+    for (int q = w.g.rank(); q < nt; q += w.g.size()) {
+      s.step_key[q] = split(chain_key, (uint32_t)(t0 + q));
+      s.step_move[q] = choice(split(move_key, (uint32_t)(t0 + q)), P.moves.cum_probs,
+                              P.moves.n_moves);
+    }
+    w.g.sync();
+    for (int t = 0; t < nt; ++t)
+      mwg_step<kExt>(P, w, s.step_key[t], s.step_move[t], emax, pressure, mu);
+    w.g.sync();
+  }
 }
 
 // Copy the about-to-be-culled walker of replica p into info row `row`, cull

@@ -20,6 +20,7 @@
 namespace jr {
 
 constexpr int kMaxWarps = 32;
+constexpr int kStepChunk = 64;  // steps whose keys and moves are drawn at once
 constexpr int kPairMatMax = 96;  // walkers up to this size use the pair matrix
                                  // (12 n (n|1) bytes: 112 KB at 96; measured faster than
                                  // the ordered pairs from 32 to 96 atoms)
@@ -117,6 +118,10 @@ struct WalkShared {
   int c_rr[JR_MAX_MOVES * 4];
   int c_nev[JR_MAX_MOVES];
   int c_ngr[JR_MAX_MOVES];
+  // step keys and move choices of the next steps of a chain
+  Key step_key[kStepChunk];
+  int step_move[kStepChunk];
+  int cell_ok;  // cell-geometry verdict of the pending cell move
   // pre-move copy for the constraint gate
   double E_save;
   int cur_save;
@@ -906,7 +911,7 @@ __device__ __forceinline__ bool move_galilean(const JrParams& P, Walker<G>& w, K
       arr.dir[q] = -arr.dp[q];
     }
   }
-  w.g.sync();
+  // every thread read s.E before the trajectory's barriers
   if (w.g.leader()) w.s.E = acc ? E : E0;
   w.g.sync();
   return acc;
@@ -969,12 +974,15 @@ __device__ __forceinline__ bool move_volume(const JrParams& P, Walker<G>& w, Key
     arr.x0[q] = x;
     x = __fmul_rn(x, scale);
   }
-  w.g.sync();
+  // the trial cell context and the cell-geometry check, side by side on two
+  // threads (of different warps when the group has them)
+  const int helper = gs > 32 ? 32 : 1;
   if (w.g.leader()) make_cell_ctx(nc, s.cc[tr], arr.T + tr * 3 * P.model.n_images, P.model);
+  else if (r0 == helper % gs) s.cell_ok = cell_valid(nc, n, mv) ? 1 : 0;
   w.g.sync();
   double d0, d1;
   const double En = ham_eval<false>(P, w, tr, pressure, mu, d0, d1);
-  const bool valid = cell_valid(nc, n, mv);
+  const bool valid = s.cell_ok != 0;
   const float u = uniform01(bits32(k2, 0u));
   bool prior_ok;
   if (mv.flat_v_prior) {
@@ -1001,7 +1009,8 @@ __device__ __forceinline__ bool move_volume(const JrParams& P, Walker<G>& w, Key
   if (!acc) {
     for (int q = r0; q < n3; q += gs) pos_at(arr.xs, q) = arr.x0[q];
   }
-  w.g.sync();
+  // cur and tr are held in registers; nothing reads s.cur or s.E before this
+  // barrier
   if (w.g.leader() && acc) {
     s.cur = tr;
     s.E = En;
@@ -1362,11 +1371,9 @@ __device__ __forceinline__ bool gated_move(const JrParams& P, Walker<G>& w, int 
 // MWG step (mwg.py:227-257 with the _wrap counters of mwg.py:108-150) plus
 // the ns_step scan-body counters (nested_sampling.py:541-609).
 template <bool kExt, class G>
-__device__ __forceinline__ void mwg_step(const JrParams& P, Walker<G>& w, Key step_key,
-                                         Key move_key, double emax, float pressure,
-                                         const float* mu) {
+__device__ __forceinline__ void mwg_step(const JrParams& P, Walker<G>& w, Key step_key, int idx,
+                                         double emax, float pressure, const float* mu) {
   WalkShared& s = w.s;
-  const int idx = choice(move_key, P.moves.cum_probs, P.moves.n_moves);
   int reason = 0;
   const bool acc = gated_move<kExt>(P, w, idx, step_key, s.step_sizes[idx], emax, pressure, mu,
                                    reason);
