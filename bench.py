@@ -355,63 +355,76 @@ def end_to_end(args, ns, step, re, cfg, torch, nsm):
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": n}
 
 
-def _oracle_reference_run(seed: int, n_iter: int, threads: int):
-    """The reference algorithm on host cores (float32, reference op order)."""
-    from jaxrens_b200 import prior_mass
-    from oracle import oracle as O
-    from tests._cases import oracle_model, oracle_moves
+class ReferenceRun:
+    """The reference algorithm on host cores: the CPU oracle in the
+    reference's float32 op order, the 8 runs threaded.  The case is built
+    once; ``iterate(n)`` advances every run by n NS iterations and returns
+    the seconds it took."""
 
-    H, init_fn, step, pos, cells, types, run_keys, _ = build_case(seed)
-    model, moves = oracle_model(H), oracle_moves(step)
-    reps = []
-    for r in range(P_RUNS):
-        e = np.array([O.energy(model, pos[r][k], types[r][k], cells[r][k],
-                               pressure=float(PRESSURES[r]), mode=O.REF32, forces=False)[0]
-                      for k in range(K)])
-        reps.append(O.Replica(pos[r], types[r], e, cells[r],
-                              np.tile(step.default_step_sizes, (K, 1)), run_keys[r],
-                              pressure=float(PRESSURES[r])))
-    la = prior_mass.log_alpha(K, 1)
-    wo = float(prior_mass.iteration_offsets(K, 1)[1][0])
-    # prologue past the random-gas start, then the timed sample
-    for _ in range(5):
-        O.ns_step_batched(model, moves, reps, T, la, wo, shared_move_key=True,
-                          mode=O.REF32, n_threads=threads)
-    t0 = time.perf_counter()
-    for _ in range(n_iter):
-        O.ns_step_batched(model, moves, reps, T, la, wo, shared_move_key=True,
-                          mode=O.REF32, n_threads=threads)
-    dt = time.perf_counter() - t0
-    return P_RUNS * T * n_iter / dt, dt
+    def __init__(self, seed: int, threads: int):
+        from jaxrens_b200 import prior_mass
+        from oracle import oracle as O
+        from tests._cases import oracle_model, oracle_moves
+
+        H, init_fn, step, pos, cells, types, run_keys, _ = build_case(seed)
+        self.O, self.threads = O, threads
+        self.model, self.moves = oracle_model(H), oracle_moves(step)
+        self.reps = []
+        for r in range(P_RUNS):
+            e = np.array([O.energy(self.model, pos[r][k], types[r][k], cells[r][k],
+                                   pressure=float(PRESSURES[r]), mode=O.REF32, forces=False)[0]
+                          for k in range(K)])
+            self.reps.append(O.Replica(pos[r], types[r], e, cells[r],
+                                       np.tile(step.default_step_sizes, (K, 1)), run_keys[r],
+                                       pressure=float(PRESSURES[r])))
+        self.la = prior_mass.log_alpha(K, 1)
+        self.wo = float(prior_mass.iteration_offsets(K, 1)[1][0])
+        self.iterate(5)  # past the random-gas start, untimed
+
+    def iterate(self, n: int) -> float:
+        t0 = time.perf_counter()
+        for _ in range(n):
+            self.O.ns_step_batched(self.model, self.moves, self.reps, T, self.la, self.wo,
+                                   shared_move_key=True, mode=self.O.REF32,
+                                   n_threads=self.threads)
+        return time.perf_counter() - t0
 
 
 def cpu_baseline(args):
     threads = min(os.cpu_count() or 1, P_RUNS)
-    val, dt = _oracle_reference_run(args.seed, args.cpu_iters, threads)
-    return {"value": val, "unit": "walker-steps/s", "cores": threads, "kind": "port",
+    dt = ReferenceRun(args.seed, threads).iterate(args.cpu_iters)
+    return {"value": P_RUNS * T * args.cpu_iters / dt, "unit": "walker-steps/s",
+            "cores": threads, "kind": "port",
             "sample": f"{args.cpu_iters} NS iterations x {P_RUNS} runs (after 5 untimed), "
                       f"{dt:.1f} s, CPU oracle in the reference's float32 op order"}
 
 
 def run_reference(args):
+    """Reference arm: each step is a bounded sample of the workload (every run
+    advanced by cpu_iters / steps NS iterations), warm-up steps untimed."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     threads = min(os.cpu_count() or 1, P_RUNS)
-    vals = []
-    for _ in range(max(1, args.steps)):
-        v, _ = _oracle_reference_run(args.seed, max(1, args.cpu_iters // max(1, args.steps)), threads)
-        vals.append(v)
-    value = float(np.mean(vals))
+    ref = ReferenceRun(args.seed, threads)
+    per_step = max(1, args.cpu_iters // max(1, args.steps))
+    for _ in range(args.warmup):
+        ref.iterate(per_step)
+    dt = sum(ref.iterate(per_step) for _ in range(max(1, args.steps)))
+    n_iter = per_step * max(1, args.steps)
+    value = P_RUNS * T * n_iter / dt
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "walker-steps/s",
-        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * dt / max(1, args.steps), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": dict(CONFIG, parallelism=f"{threads} host threads over runs"),
         "cpu_baseline": {"value": value, "unit": "walker-steps/s", "cores": threads,
                          "kind": "port",
-                         "sample": "reference algorithm (CPU oracle, reference float32 op order); "
-                                   "JAX is not installable on this image"},
+                         "sample": f"{per_step} NS iterations x {P_RUNS} runs per step, "
+                                   f"{dt:.1f} s timed; reference algorithm (CPU oracle, "
+                                   "reference float32 op order); JAX is not installable on "
+                                   "this image"},
         "e2e": {"value": value, "unit": "walker-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
