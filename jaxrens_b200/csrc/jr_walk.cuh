@@ -814,10 +814,19 @@ __device__ __forceinline__ double galilean_trajectory(const JrParams& P, Walker<
   if (kPath != kTrajModel) cc = load_mic<kDiag>(w.s.cc[cidx]);
   const float* T = arr.T + cidx * 3 * P.model.n_images;
   double E = w.s.E;
+  // a reflection off the contour is applied by the coordinate's owner thread
+  // together with the next position update (d is reused from the register)
+  bool refl = false;
+  float coef = 0.0f;
   for (int r = 0; r < R; ++r) {
     for (int q = r0; q < n3; q += gs) {
+      float d = arr.dir[q];
+      if (refl) {
+        d = __fmaf_rn(-coef, arr.F[q], d);
+        arr.dir[q] = d;
+      }
       float& x = pos_at(arr.xs, q);
-      x = __fmaf_rn(step, arr.dir[q], x);
+      x = __fmaf_rn(step, d, x);
     }
     w.g.sync();
     double U, sff, sfd;
@@ -832,13 +841,15 @@ __device__ __forceinline__ double galilean_trajectory(const JrParams& P, Walker<
       E = U;
     }
     if (isnan(E)) E = INFINITY;
-    if (E >= emax) {
+    refl = E >= emax;
+    if (refl) {
       // d <- d - [2 (F.d) / max(|F|^2, 1e-20)] F, the scalar in float32
       const float ffs = __double2float_rn(sff);
-      const float coef = __fmul_rn(2.0f * __double2float_rn(sfd), rcp_nr(ffs > 1e-20f ? ffs : 1e-20f));
-      for (int q = r0; q < n3; q += gs) arr.dir[q] = __fmaf_rn(-coef, arr.F[q], arr.dir[q]);
+      coef = __fmul_rn(2.0f * __double2float_rn(sfd), rcp_nr(ffs > 1e-20f ? ffs : 1e-20f));
     }
   }
+  if (refl)
+    for (int q = r0; q < n3; q += gs) arr.dir[q] = __fmaf_rn(-coef, arr.F[q], arr.dir[q]);
   return E;
 }
 
