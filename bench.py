@@ -44,6 +44,48 @@ CONFIG = {
     "n_reflect": R_REFLECT, "re_interval": RE_INTERVAL, "n_cull": 1, "n_extra": 0,
     "iterations_per_step": RE_INTERVAL,
 }
+# per-run atom counts and chemical potentials (the uneven semi-grand workload)
+N_LIST = [N] * P_RUNS
+MUS = None
+RE_ON = True
+WORKLOAD = "batched"
+
+
+def select_workload(name: str) -> None:
+    """The default is the batched-replica configuration above.  ``single``:
+    one 8-atom LJ NPT run (P = 0.1) of 128 walkers, n_mcmc_steps = 20.
+    ``uneven``: 16 semi-grand runs of binary LJ (sigma AA/BB/AB 1/0.88/0.8,
+    epsilon 1/0.5/1.5, cutoff 2.5) with atom counts drawn from {16, 24, ..., 96}
+    (seeded), Delta-mu signed-log-spaced in [-2, 2], 1024 walkers, species
+    Bernoulli(0.5), galilean + volume + morph + swap, n_mcmc_steps = 40, all runs
+    in one launch.  Neither exchanges replicas; a step is 10 NS iterations."""
+    global P_RUNS, K, N, T, PRESSURES, CONFIG, N_LIST, MUS, RE_ON, WORKLOAD
+    WORKLOAD = name
+    if name == "batched":
+        return
+    RE_ON = False
+    if name == "single":
+        P_RUNS, K, N, T = 1, 128, 8, 20
+        N_LIST = [N]
+        PRESSURES = np.full(1, 0.1, np.float32)
+        desc = ("LJ-8 NPT single run (P=0.1) x 128 walkers, n_mcmc_steps=20, "
+                "galilean(n_reflect=10)+volume")
+    elif name == "uneven":
+        P_RUNS, K, T = 16, 1024, 40
+        N_LIST = [int(v) for v in np.random.default_rng(96).choice(np.arange(16, 97, 8), 16)]
+        N = max(N_LIST)
+        PRESSURES = np.full(P_RUNS, 0.1, np.float32)
+        dmu = np.concatenate([-np.logspace(np.log10(2.0), -2, 8), np.logspace(-2, np.log10(2.0), 8)])
+        MUS = np.stack([np.zeros(P_RUNS), dmu], axis=1).astype(np.float32)
+        desc = ("binary LJ semi-grand (Kob-Andersen pair tables), 16 runs with N in "
+                "{16..96} x 1024 walkers, Delta-mu in [-2, 2], n_mcmc_steps=40, "
+                "galilean(n_reflect=10)+volume+morph+swap")
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    CONFIG = {"workload": desc, "n_runs": P_RUNS, "n_walkers": K,
+              "n_atoms": N_LIST if name == "uneven" else N, "n_mcmc_steps": T,
+              "n_reflect": R_REFLECT, "re_interval": None, "n_cull": 1, "n_extra": 0,
+              "iterations_per_step": RE_INTERVAL}
 # algorithmic flops per unique pair interaction (triclinic MIC accounting)
 FLOPS_EF, FLOPS_E = 61.0, 48.0
 
@@ -53,19 +95,29 @@ def build_case(seed: int):
     from jaxrens_b200 import init as jinit
     from jaxrens_b200 import moves as mvs
 
-    lj = create_lj(epsilon=1.0, sigma=1.0, cutoff=2.5)
+    if WORKLOAD == "uneven":
+        lj = create_lj(epsilon=[[1.0, 1.5], [1.5, 0.5]], sigma=[[1.0, 0.8], [0.8, 0.88]],
+                       cutoff=2.5)
+    else:
+        lj = create_lj(epsilon=1.0, sigma=1.0, cutoff=2.5)
     H = Hamiltonian(lj, [EnsembleTerm(pressure=0.1)])
     moves = [mvs.gmc(n_reflect=R_REFLECT, step_size=0.1, weight=4.0),
              mvs.volume_move(N, step_size=0.3, weight=1.0)]
+    if WORKLOAD == "uneven":
+        moves += [mvs.morph_move(2, weight=1.0), mvs.swap_move(2, weight=1.0)]
     init_fn, step, _ = build_mwg(H, moves)
     root = prng.key(seed)
     keys = prng.split(root, P_RUNS + 2)
     pos, cells = [], []
     for r in range(P_RUNS):
-        p_, c_ = jinit.uniform_gas(keys[r], K, N, 8.0 * N)
+        p_, c_ = jinit.uniform_gas(keys[r], K, N_LIST[r], 8.0 * N_LIST[r])
         pos.append(p_)
         cells.append(c_)
-    types = [np.zeros((K, N), np.int32) for _ in range(P_RUNS)]
+    if WORKLOAD == "uneven":
+        rng = np.random.default_rng(seed)
+        types = [rng.integers(0, 2, size=(K, n)).astype(np.int32) for n in N_LIST]
+    else:
+        types = [np.zeros((K, N), np.int32) for _ in range(P_RUNS)]
     run_keys = prng.split(keys[P_RUNS], P_RUNS)
     return H, init_fn, step, pos, cells, types, run_keys, keys[P_RUNS + 1]
 
@@ -175,10 +227,10 @@ def job_throughput(world: int, iters: int, total_ms: float) -> tuple[float, floa
 def algorithmic_flops(info) -> float:
     """Sum over the launch's committed iterations of eval counts x unique
     pairs x flops per pair (61 energy+forces, 48 energy-only)."""
-    pairs = N * (N - 1) / 2.0
-    ne = info.n_evaluations.sum().item()
-    ng = info.n_grad_evaluations.sum().item()
-    return (ng * FLOPS_EF + (ne - ng) * FLOPS_E) * pairs
+    pairs = np.array([n * (n - 1) / 2.0 for n in N_LIST])
+    ne = info.n_evaluations.sum(dim=(0, 2)).cpu().numpy()  # per run
+    ng = info.n_grad_evaluations.sum(dim=(0, 2)).cpu().numpy()
+    return float(np.sum((ng * FLOPS_EF + (ne - ng) * FLOPS_E) * pairs))
 
 
 def run_ours(args):
@@ -199,6 +251,8 @@ def run_ours(args):
 
     H, init_fn, step, pos, cells, types, run_keys, re_key = build_case(rank_seed(args.seed, rank))
     pr = {"pressure": PRESSURES}
+    if MUS is not None:
+        pr["chemical_potentials"] = MUS
     ns = nsm.init_ns_parallel(init_fn, pos, types, None, cells, run_keys, ensemble_params=pr)
     re = nsm.InterREManager(RE_INTERVAL, 1, re_key)
     cfg = None
@@ -218,7 +272,8 @@ def run_ours(args):
     info = nsm.InfoBuffers(ns, step.n_moves, RE_INTERVAL, dead=True)
     for _ in range(args.prologue // RE_INTERVAL):
         nsm.ns_iterate(ns, step, RE_INTERVAL, T, 0, info=info, cfg=cfg)
-        re.apply(ns, step)
+        if RE_ON:
+            re.apply(ns, step)
     torch.cuda.synchronize()
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -229,7 +284,8 @@ def run_ours(args):
         nsm.ns_iterate(ns, step, RE_INTERVAL, T, 0, info=info, cfg=cfg)
         if record is not None:
             record[1].record()
-        re.apply(ns, step)
+        if RE_ON:
+            re.apply(ns, step)
 
     for _ in range(args.warmup):
         one_step(None)
@@ -274,7 +330,7 @@ def run_ours(args):
     cpu = cpu_baseline(args) if (world == 1 and not args.no_cpu) else None
     traffic = None
     prof = os.path.join(ROOT, "profiles", "ns_iterate_kernel_lj32_8x512.json")
-    if os.path.exists(prof):
+    if WORKLOAD == "batched" and os.path.exists(prof):
         traffic = json.load(open(prof)).get("dram_bytes_per_launch")
     line = {
         "metric": METRIC, "value": value, "unit": "walker-steps/s", "n_gpus": world,
@@ -363,7 +419,8 @@ def end_to_end(args, ns, step, re, cfg, torch, nsm):
             upload(k + 1)
         main.wait_event(uploaded[b])
         nsm.ns_iterate(bufs[b][1], step, RE_INTERVAL, T, 0, info=info, cfg=cfg)
-        re.apply(bufs[b][1], step)
+        if RE_ON:
+            re.apply(bufs[b][1], step)
         consumed[b].record(main)
         out_e.copy_(info.emax, non_blocking=True)
         out_z.copy_(info.log_evidence, non_blocking=True)
@@ -392,12 +449,14 @@ class ReferenceRun:
         self.model, self.moves = oracle_model(H), oracle_moves(step)
         self.reps = []
         for r in range(P_RUNS):
+            mu = None if MUS is None else MUS[r]
             e = np.array([O.energy(self.model, pos[r][k], types[r][k], cells[r][k],
-                                   pressure=float(PRESSURES[r]), mode=O.REF32, forces=False)[0]
+                                   pressure=float(PRESSURES[r]), mu=mu, mode=O.REF32,
+                                   forces=False)[0]
                           for k in range(K)])
             self.reps.append(O.Replica(pos[r], types[r], e, cells[r],
                                        np.tile(step.default_step_sizes, (K, 1)), run_keys[r],
-                                       pressure=float(PRESSURES[r])))
+                                       pressure=float(PRESSURES[r]), mu=mu))
         self.la = prior_mass.log_alpha(K, 1)
         self.wo = float(prior_mass.iteration_offsets(K, 1)[1][0])
         self.iterate(5)  # past the random-gas start, untimed
@@ -467,7 +526,11 @@ def main():
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--tpa", type=int, default=8)
     ap.add_argument("--warp", type=int, default=0)
+    ap.add_argument("--workload", default="batched", choices=["batched", "single", "uneven"],
+                    help="batched (default, the headline line), or the single-run and uneven "
+                         "semi-grand configurations")
     args = ap.parse_args()
+    select_workload(args.workload)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
