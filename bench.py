@@ -365,11 +365,14 @@ def run_ours(args):
 
 
 def end_to_end(args, ns, step, re, cfg, torch, nsm):
-    """Each step: the pinned-host state -> device (one copy), 10 iterations +
+    """Each step: a pinned-host state -> device (one copy), 10 iterations +
     swap through the public API, per-iteration results (dead energies, log Z)
-    -> host.  Two device copies of the state alternate, so the upload of step
-    k+1 (on a copy stream) overlaps the walk of step k; every step still
-    starts from its own upload."""
+    -> host.  The host holds n_snap consecutive states of the run and step k
+    starts from state k mod n_snap, so the steps sample different trajectories
+    (and speculation outcomes) as the device-resident steps do.  Two device
+    copies of the state alternate, so the upload of step k+1 (on a copy
+    stream) overlaps the walk of step k; every step starts from its own
+    upload."""
     import dataclasses
 
     pop = ns.population
@@ -385,10 +388,6 @@ def end_to_end(args, ns, step, re, cfg, torch, nsm):
         off = (off + 255) // 256 * 256
         offs.append(off)
         off += f.numel() * f.element_size()
-    flat_host = torch.zeros(off, dtype=torch.uint8).pin_memory()
-    for f, o in zip(fields, offs):
-        nb = f.numel() * f.element_size()
-        flat_host[o:o + nb].copy_(f.detach().contiguous().view(-1).view(torch.uint8).cpu())
     bufs = []
     for _ in range(2):
         flat_dev = torch.empty(off, dtype=torch.uint8, device=pop.positions.device)
@@ -399,10 +398,25 @@ def end_to_end(args, ns, step, re, cfg, torch, nsm):
         bufs.append((flat_dev, ns_b))
     h2d = off
     info = nsm.InfoBuffers(bufs[0][1], step.n_moves, RE_INTERVAL, dead=False)
+    # consecutive states (one step apart) in pinned host memory, as many as
+    # the timed steps up to 32 (128 MB), so the end-to-end mean covers as many
+    # trajectories as the device-resident one
+    n = max(3, args.steps // 2)
+    n_snap = min(n, 32)
+    for f, v in zip(fields, [getattr(bufs[0][1].population, k) for k in names_p] +
+                    [getattr(bufs[0][1], k) for k in names_s]):
+        v.copy_(f)
+    flat_host = []
+    for _ in range(n_snap):
+        h = torch.empty(off, dtype=torch.uint8).pin_memory()
+        h.copy_(bufs[0][0])
+        flat_host.append(h)
+        nsm.ns_iterate(bufs[0][1], step, RE_INTERVAL, T, 0, info=info, cfg=cfg)
+        if RE_ON:
+            re.apply(bufs[0][1], step)
     out_e = torch.empty((RE_INTERVAL, P_RUNS), dtype=torch.float64).pin_memory()
     out_z = torch.empty((RE_INTERVAL, P_RUNS), dtype=torch.float64).pin_memory()
     d2h = out_e.numel() * 8 + out_z.numel() * 8
-    n = max(3, args.steps // 2)
     main = torch.cuda.current_stream()
     copy = torch.cuda.Stream()
     uploaded = [torch.cuda.Event(), torch.cuda.Event()]
@@ -412,7 +426,7 @@ def end_to_end(args, ns, step, re, cfg, torch, nsm):
         b = k % 2
         with torch.cuda.stream(copy):
             copy.wait_event(consumed[b] if k >= 2 else t0)
-            bufs[b][0].copy_(flat_host, non_blocking=True)
+            bufs[b][0].copy_(flat_host[k % n_snap], non_blocking=True)
             uploaded[b].record(copy)
 
     torch.cuda.synchronize()
@@ -437,7 +451,8 @@ def end_to_end(args, ns, step, re, cfg, torch, nsm):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     return {"value": world * P_RUNS * T * RE_INTERVAL * n / (ms * 1e-3), "unit": "walker-steps/s",
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": n,
-            "pipeline": "state upload of step k+1 on a copy stream overlaps the walk of step k"}
+            "pipeline": "state upload of step k+1 on a copy stream overlaps the walk of step k",
+            "inputs": f"{n_snap} consecutive host states of the run, cycled"}
 
 
 class ReferenceRun:
