@@ -300,20 +300,29 @@ __device__ void predict_fast(NsShared& ns, const double* E, int K, int Dr, Key k
   uint32_t taken = 0;
   bool prev_ok = true;
   double prev_e = 0.0;
-  for (int d = 0; d < Dr; ++d) {
-    unsigned long long best = 0;
-    int nanf = 0;
+  // this lane's largest non-culled energy (ordered bits) and NaN flag; only
+  // the lane that loses a walker to a cull rescans its entries
+  unsigned long long lbest = 0;
+  int lnan = 0;
+  auto lane_scan = [&]() {
+    lbest = 0;
+    lnan = 0;
     for (int j = 0; j < nslot; ++j) {
       const int k = lane + 32 * j;
       if (k >= K || ((taken >> j) & 1u)) continue;
       const double x = E[k];
       if (isnan(x)) {
-        nanf = 1;
+        lnan = 1;
       } else {
         const unsigned long long o = ord_double(x);
-        best = o > best ? o : best;
+        lbest = o > lbest ? o : lbest;
       }
     }
+  };
+  lane_scan();
+  for (int d = 0; d < Dr; ++d) {
+    unsigned long long best = lbest;
+    int nanf = lnan;
     for (int off = 16; off > 0; off >>= 1) {
       const unsigned long long o = __shfl_xor_sync(0xffffffffu, best, off);
       best = o > best ? o : best;
@@ -324,21 +333,45 @@ __device__ void predict_fast(NsShared& ns, const double* E, int K, int Dr, Key k
     double emax = __longlong_as_double(0x7ff8000000000000ll);
     if (!any_nan) {
       emax = unord_double(best);
-      const Key kw{__shfl_sync(0xffffffffu, my_kw.k0, d), __shfl_sync(0xffffffffu, my_kw.k1, d)};
-      unsigned long long tb = 0;
-      for (int j = 0; j < nslot; ++j) {
-        const int k = lane + 32 * j;
-        if (k >= K || ((taken >> j) & 1u) || E[k] != emax) continue;
-        const float nz = uniform01(bits32(kw, (uint32_t)k));
-        const unsigned long long t =
-            ((unsigned long long)__float_as_uint(nz) << 32) | (0xFFFFFFFFu - (unsigned)k);
-        tb = t > tb ? t : tb;
+      // walkers at the maximum: a unique one is the cull whatever the noise;
+      // exact ties are broken by the largest noise of this iteration's key
+      int nties = 0, idx1 = 0;
+      // (== on the values: -0.0 ties with +0.0, as in the reference's E == max)
+      if (lbest != 0 && unord_double(lbest) == emax) {
+        for (int j = 0; j < nslot; ++j) {
+          const int k = lane + 32 * j;
+          if (k >= K || ((taken >> j) & 1u) || E[k] != emax) continue;
+          ++nties;
+          idx1 = k + 1;
+        }
       }
+      int tot = nties, idx = idx1;
       for (int off = 16; off > 0; off >>= 1) {
-        const unsigned long long o = __shfl_xor_sync(0xffffffffu, tb, off);
-        tb = o > tb ? o : tb;
+        tot += __shfl_xor_sync(0xffffffffu, tot, off);
+        const int o = __shfl_xor_sync(0xffffffffu, idx, off);
+        idx = o > idx ? o : idx;
       }
-      worst = (int)(0xFFFFFFFFu - (unsigned)(tb & 0xFFFFFFFFull));
+      if (tot == 1) {
+        worst = idx - 1;
+      } else {
+        const Key kw{__shfl_sync(0xffffffffu, my_kw.k0, d), __shfl_sync(0xffffffffu, my_kw.k1, d)};
+        unsigned long long tb = 0;
+        if (nties > 0) {
+          for (int j = 0; j < nslot; ++j) {
+            const int k = lane + 32 * j;
+            if (k >= K || ((taken >> j) & 1u) || E[k] != emax) continue;
+            const float nz = uniform01(bits32(kw, (uint32_t)k));
+            const unsigned long long t =
+                ((unsigned long long)__float_as_uint(nz) << 32) | (0xFFFFFFFFu - (unsigned)k);
+            tb = t > tb ? t : tb;
+          }
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+          const unsigned long long o = __shfl_xor_sync(0xffffffffu, tb, off);
+          tb = o > tb ? o : tb;
+        }
+        worst = (int)(0xFFFFFFFFu - (unsigned)(tb & 0xFFFFFFFFull));
+      }
     }
     int clone = __shfl_sync(0xffffffffu, my_raw, d);
     if (clone >= worst) clone += 1;
@@ -346,7 +379,10 @@ __device__ void predict_fast(NsShared& ns, const double* E, int K, int Dr, Key k
     const unsigned cbit = __shfl_sync(0xffffffffu, taken, clone & 31);
     const bool conflict = d > 0 && ((cbit >> (clone >> 5)) & 1u);
     const bool sp = d == 0 || (prev_ok && !any_nan && !isnan(prev_e) && !conflict);
-    if (lane == (worst & 31)) taken |= 1u << (worst >> 5);
+    if (lane == (worst & 31)) {
+      taken |= 1u << (worst >> 5);
+      if (d + 1 < Dr) lane_scan();
+    }
     if (lane == 0) {
       ns.spec[d] = sp ? 1 : 0;
       ns.worst[d] = worst;
@@ -598,19 +634,22 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
         store_walker(D, st, w, p, dst);
       }
     }
-    // ---- per-iteration info and replica scalars (CTA 0) ----
-    if (c == 0 && threadIdx.x == 0) {
-      int it = iter;
-      for (int d = 0; d < nval; ++d, ++it) {
-        const size_t ib = (size_t)(committed + d) * D.n_replicas + p;
-        const int s0 = Dmax == 1 ? 0 : d * W;
-        const int s1 = Dmax == 1 ? (slots < W ? slots : W) : d * W + W;
+    // ---- per-iteration move counters: the group that walked the first slot
+    // of a committed iteration sums that iteration's slots and writes them
+    // (its own slot from local shared memory), all iterations in parallel ----
+    {
+      const int d_own = Dmax == 1 ? (s_my == 0 ? 0 : -1)
+                                  : ((s_my % W == 0 && s_my / W < nval) ? s_my / W : -1);
+      if (d_own >= 0 && w.g.leader()) {
+        const size_t ib = (size_t)(committed + d_own) * D.n_replicas + p;
+        const int s0 = Dmax == 1 ? 0 : d_own * W;
+        const int s1 = Dmax == 1 ? (slots < W ? slots : W) : d_own * W + W;
         for (int m = 0; m < M; ++m) {
           int a = 0, pr = 0, ne = 0, ng = 0, rr[4] = {0, 0, 0, 0};
           for (int sl = s0; sl < s1; ++sl) {
             const WalkShared* local = reinterpret_cast<const WalkShared*>(
                 L.walkers + (size_t)(sl % cpc) * L.walker_bytes);
-            const WalkShared* rs = cluster.map_shared_rank(local, sl / cpc);
+            const WalkShared* rs = sl == s_my ? local : cluster.map_shared_rank(local, sl / cpc);
             a += rs->c_acc[m];
             pr += rs->c_prop[m];
             ne += rs->c_nev[m];
@@ -624,6 +663,13 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
           if (info.reject_reason_counts)
             for (int q = 0; q < 4; ++q) info.reject_reason_counts[(ib * M + m) * 4 + q] = rr[q];
         }
+      }
+    }
+    // ---- per-iteration culls, evidence and replica scalars (CTA 0) ----
+    if (c == 0 && threadIdx.x == 0) {
+      int it = iter;
+      for (int d = 0; d < nval; ++d, ++it) {
+        const size_t ib = (size_t)(committed + d) * D.n_replicas + p;
         if (ncull == 1) {
           const double lw = (double)it * P.log_alpha + P.w_offset[0];
           logZ = logaddexp(logZ, lw - ns.e[d]);
@@ -652,9 +698,18 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
         if (info.log_evidence) info.log_evidence[ib] = logZ;
       }
     }
-    for (int d = 0; d < nval; ++d) {
-      key = advance_iteration(key);
-      key0 = advance_iteration(key0);
+    if (fast) {
+      // the predictions stored the chain: kchain[d] is the key after d
+      // iterations, so the committed key is one advance past kchain[nval-1]
+      key = advance_iteration(ns.kchain[nval - 1]);
+      if (D.shared_move_key) key0 = advance_iteration(ns.k0chain[nval - 1]);
+      else
+        for (int d = 0; d < nval; ++d) key0 = advance_iteration(key0);
+    } else {
+      for (int d = 0; d < nval; ++d) {
+        key = advance_iteration(key);
+        key0 = advance_iteration(key0);
+      }
     }
     if (c == 0 && threadIdx.x == 0) {
       st.emax[p] = ns.e[nval - 1];
