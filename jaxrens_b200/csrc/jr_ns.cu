@@ -1080,18 +1080,22 @@ bool spec_fits(const JrLaunchConfig& c, const JrDims* d) {
   return D * d->n_extra <= jr::kMaxWalk && D * W <= jr::kMaxWalk;
 }
 
-// Default shape of the NS launch: a CTA per walker chain (256 threads) for
-// 16 < N <= 64, warp walkers for N <= 16.  The cluster serves the speculative
+// Default shape of the NS launch: a CTA per walker chain, 128 threads for
+// N <= 16, 256 for N <= 64, 512 above (measured: a 128-thread CTA walks an
+// 8-atom chain 8% faster than a warp).  The cluster serves the speculative
 // iterations of one run: no more CTAs than one launch's n_iter * (1 + n_extra)
-// chains can use, at most 10 (larger clusters were measured to share SMs
-// between their CTAs, which slows every chain), and a grid under about 55% of
-// the SMs for the same reason.
+// chains can use, and at most 10 (clusters of 12-16 were measured to share
+// SMs between their CTAs, which slows every chain).  A cluster that covers
+// the launch's iterations commits them in about one round, which outweighs a
+// grid somewhat larger than the SM count (16 runs of 1024 walkers with up to
+// 96 atoms: clusters of 10, 160 CTAs, walked 1.4x faster than clusters of 8
+// or 9), so the grid is capped at 1.2x the SMs.
 JrLaunchConfig ns_heuristic_config(const JrDims* d, int n_iter) {
   JrLaunchConfig c = heuristic_config(d);
   const int nmax = d->n_atoms_max;
-  if (nmax > 16 && nmax <= 64) {
+  if (nmax <= 64) {
     c.warp_walkers = 0;
-    c.threads = 256;
+    c.threads = nmax <= 16 ? 128 : 256;
     const int tpa = pow2_floor(c.threads / nmax);
     c.tpa = tpa > 16 ? 16 : (tpa < 1 ? 1 : tpa);
   }
@@ -1107,7 +1111,7 @@ JrLaunchConfig ns_heuristic_config(const JrDims* d, int n_iter) {
   // otherwise the W chains of one iteration
   const int want = d->n_cull > 1 ? W : (n_iter > 0 ? n_iter : 1) * W;
   int cl = (want + cpc - 1) / cpc;
-  const int fit = (sms * 11 / 20) / (d->n_replicas > 0 ? d->n_replicas : 1);
+  const int fit = (sms * 6 / 5) / (d->n_replicas > 0 ? d->n_replicas : 1);
   if (cl > 10) cl = 10;
   if (cl > fit) cl = fit;
   if (cl < 1) cl = 1;
