@@ -492,11 +492,25 @@ class ReferenceRun:
         return time.perf_counter() - t0
 
 
+def host_cpu() -> dict:
+    """The host's logical CPU count and model name (from /proc/cpuinfo)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"host_cpus": os.cpu_count(), "cpu_model": model}
+
+
 def cpu_baseline(args):
     threads = min(os.cpu_count() or 1, P_RUNS)
     dt = ReferenceRun(args.seed, threads).iterate(args.cpu_iters)
     return {"value": P_RUNS * T * args.cpu_iters / dt, "unit": "walker-steps/s",
-            "cores": threads, "kind": "port",
+            "cores": threads, "kind": "port", **host_cpu(),
             "sample": f"{args.cpu_iters} NS iterations x {P_RUNS} runs (after 5 untimed), "
                       f"{dt:.1f} s, CPU oracle in the reference's float32 op order"}
 
@@ -522,7 +536,7 @@ def run_reference(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": dict(CONFIG, parallelism=f"{threads} host threads over runs"),
         "cpu_baseline": {"value": value, "unit": "walker-steps/s", "cores": threads,
-                         "kind": "port",
+                         "kind": "port", **host_cpu(),
                          "sample": f"{per_step} NS iterations x {P_RUNS} runs per step, "
                                    f"{dt:.1f} s timed; reference algorithm (CPU oracle, "
                                    "reference float32 op order); JAX is not installable on "
