@@ -64,7 +64,7 @@ enum {
   JR_ERR_CUDA = -3,        /* a CUDA runtime call failed */
   JR_ERR_TIMEOUT = -4,     /* a bounded device-side wait gave up */
   JR_ERR_WORKSPACE = -5,   /* workspace missing or too small */
-  JR_ERR_UNSUPPORTED = -6  /* feature outside this build */
+  JR_ERR_UNSUPPORTED = -6  /* a feature the library does not implement */
 };
 
 enum { JR_MODEL_LJ = 0, JR_MODEL_GAUSS_MIX = 1 };

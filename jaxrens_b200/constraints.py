@@ -45,7 +45,7 @@ def move_gates(constraints, move_descriptors) -> tuple[list[int], np.ndarray | N
     relevant = []
     for c in constraints:
         if c.name != "minimum_distance":
-            raise NotImplementedError(f"constraint {c.name!r} has no kernel in this build")
+            raise NotImplementedError(f"constraint {c.name!r} has no CUDA kernel in this library")
         if dmin is not None:
             raise NotImplementedError("one minimum-distance constraint per sampler")
         dmin = np.asarray(c.build_kwargs["d_min_matrix"], np.float32)

@@ -1,4 +1,4 @@
-"""Statistical parity on the B200 (the north star's fourth check).
+"""Statistical parity on the B200: log Z and C_v against independent runs.
 
 * Gaussian-mixture toy (backends/toy.py:163-204): the evidence of GPU runs
   matches the analytic log Z on its uniform prior cube.
