@@ -512,6 +512,7 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
   WalkShared* wsp = carve_walker(L.walkers + (size_t)my * L.walker_bytes, D.n_atoms_max, nimg,
                                  L.pij, arr);
   Walker<G> w{*wsp, arr, tab, n, tpa, make_group<G>(red), 0};
+  zero_pair_matrix(w.g, arr, D.n_atoms_max);
   int par = 0;
   __syncthreads();
   load_tables(P, tab);
@@ -761,6 +762,7 @@ move_trial_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st, co
   const int p = t_global / n_trials;
   const int n = min(max(st.n_atoms[p], 1), D.n_atoms_max);
   Walker<G> w{*wsp, arr, tab, n, tpa, make_group<G>(red), 0};
+  zero_pair_matrix(w.g, arr, D.n_atoms_max);
   build_group_pair_table(w.g, pij, n);
   const size_t tb = (size_t)t_global;
   const int slot = walker_idx[tb];
@@ -830,6 +832,7 @@ walk_population_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers s
   const int p = t_global / K, slot = t_global % K;
   const int n = min(max(st.n_atoms[p], 1), D.n_atoms_max);
   Walker<G> w{*wsp, arr, tab, n, tpa, make_group<G>(red), 0};
+  zero_pair_matrix(w.g, arr, D.n_atoms_max);
   build_group_pair_table(w.g, pij, n);
   load_walker(P, D, st, w, p, slot, false);
   const float* mu = st.mu ? st.mu + (size_t)p * P.model.n_species : nullptr;
@@ -868,6 +871,7 @@ energy_kernel(const JrParams Pg, const int n_configs, const int nmax, const floa
   const int n = min(max(n_atoms[b], 1), nmax);
   const int smax = Pg.model.n_species - 1;
   Walker<G> w{*wsp, arr, tab, n, tpa, make_group<G>(red), 0};
+  zero_pair_matrix(w.g, arr, nmax);
   build_group_pair_table(w.g, pij, n);
   const int r0 = w.g.rank(), gs = w.g.size();
   for (int q = r0; q < 3 * n; q += gs) {

@@ -22,7 +22,7 @@ namespace jr {
 constexpr int kMaxWarps = 32;
 constexpr int kStepChunk = 64;  // steps whose keys and moves are drawn at once
 constexpr int kPairMatMax = 96;  // walkers up to this size use the pair matrix
-                                 // (12 n (n|1) bytes: 112 KB at 96; measured faster than
+                                 // (12 n pm_stride(n) bytes: 112 KB at 96; measured faster than
                                  // the ordered pairs from 32 to 96 atoms)
 
 // ------------------------------------------------------------- groups ----
@@ -148,7 +148,7 @@ struct WalkArrays {
   float* dp;            // [3 Nmax] perturbed direction (flip target on reject)
   float* F;             // [3 Nmax] forces
   float* T;             // [2][3 n_img] image translations for cc[0], cc[1]
-  float* pm;            // [3][n][n|1] pair force terms g*dr_ij, or nullptr
+  float* pm;            // [3][n][pm_stride(n)] pair force terms g*dr_ij, or nullptr
   const uint16_t* pij;  // [Nmax(Nmax-1)/2] pair decode a | b << 8, or nullptr
 };
 
@@ -157,6 +157,14 @@ __host__ __device__ inline bool use_pair_matrix(int nmax, int nimg) {
 }
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+// Row stride of the pair-force matrix: n rounded up to the 8-partner gather
+// blocks, made odd (an odd stride keeps the warp's row reads and the pair
+// stores on distinct banks).  Columns n.. and the diagonal are never written
+// by the pair loop and stay +0.0 from zero_pair_matrix, so the gather reads
+// whole blocks unconditionally: an absent partner contributes +0.0, as the
+// canonical order prescribes.
+__host__ __device__ inline int pm_stride(int n) { return ((n + 7) & ~7) | 1; }
 
 __host__ __device__ inline size_t pair_count(int nmax) {
   return (size_t)nmax * (size_t)(nmax - 1) / 2;
@@ -167,7 +175,7 @@ __host__ __device__ inline size_t walker_smem_bytes(int nmax, int nimg) {
   size_t b = align16(sizeof(WalkShared));
   b += 2u * 16u * (size_t)nmax + 4u * 12u * (size_t)nmax;
   b += align16(2u * 3u * 4u * (size_t)nimg);
-  if (use_pair_matrix(nmax, nimg)) b += align16(12u * (size_t)nmax * (size_t)(nmax | 1));
+  if (use_pair_matrix(nmax, nimg)) b += align16(12u * (size_t)nmax * (size_t)pm_stride(nmax));
   return align16(b);
 }
 
@@ -195,6 +203,15 @@ __device__ inline WalkShared* carve_walker(char* p, int nmax, int nimg, const ui
     a.pij = nullptr;
   }
   return s;
+}
+
+// Zero a walker's whole pair-force matrix (sized for nmax), group-wide; the
+// group synchronises before the first evaluation.
+template <class G>
+__device__ inline void zero_pair_matrix(const G& g, const WalkArrays& a, int nmax) {
+  if (a.pm == nullptr) return;
+  const int words = 3 * nmax * pm_stride(nmax);
+  for (int q = g.rank(); q < words; q += g.size()) a.pm[q] = 0.0f;
 }
 
 // Fill the pair decode table for n atoms (pairs a < b, row-major), CTA-wide.
@@ -517,7 +534,7 @@ __device__ __forceinline__ void pairs_matrix(const JrParams& P, Walker<G>& w, co
   const float sig2_1 = w.tab.sig2[0], eps4_1 = w.tab.eps4[0], eps24_1 = w.tab.eps24[0];
   const int np = n * (n - 1) / 2;
   const int tid = w.g.rank(), gs = w.g.size();
-  const int S = n | 1, plane = n * S;
+  const int S = pm_stride(n), plane = n * S;
   double ep = 0.0;
   // Two pairs per trip with every shared-memory load issued before any store,
   // so the pairs overlap (the compiler cannot move loads above the stores).
@@ -592,23 +609,26 @@ __device__ __forceinline__ void pairs_matrix(const JrParams& P, Walker<G>& w, co
     // warps whose atoms all lie beyond n leave the issue slots to the others
     if (!__any_sync(0xffffffffu, i < n)) continue;
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-    // partners j0..j0+7 in ascending order; an absent partner adds +0, which
-    // leaves the running sum unchanged (it is never -0).  Absent partners read
-    // a clamped in-range element, so all 24 loads issue before the adds.
+    // partners j0..j0+7 in ascending order; an absent partner (the atom
+    // itself, or a column past n) adds +0, which leaves the running sum
+    // unchanged (it is never -0); all 24 loads issue before the adds.
     const int j0 = blk * 8;
     const int ic = i < n ? i : 0;
-    const float* row = arr.pm + ic * S;
     const float d0 = arr.dir[3 * ic], d1 = arr.dir[3 * ic + 1], d2 = arr.dir[3 * ic + 2];
     float vx[8], vy[8], vz[8];
+    if (j0 < n) {
+      // partners j0..j0+7 of row i: the diagonal and the columns past n hold
+      // +0.0 (lanes of atoms past n read row 0; their sums are discarded)
+      const float* row = arr.pm + ic * S + j0;
 #pragma unroll
-    for (int jj = 0; jj < 8; ++jj) {
-      const int j = j0 + jj;
-      const bool ok = (i < n) && (j < n) && (j != i);
-      const int jc = ok ? j : ic;
-      const float x = row[jc], y = row[plane + jc], z = row[2 * plane + jc];
-      vx[jj] = ok ? x : 0.0f;
-      vy[jj] = ok ? y : 0.0f;
-      vz[jj] = ok ? z : 0.0f;
+      for (int jj = 0; jj < 8; ++jj) {
+        vx[jj] = row[jj];
+        vy[jj] = row[plane + jj];
+        vz[jj] = row[2 * plane + jj];
+      }
+    } else {
+#pragma unroll
+      for (int jj = 0; jj < 8; ++jj) vx[jj] = vy[jj] = vz[jj] = 0.0f;
     }
     if (!ep_folded) fold_ep();
 #pragma unroll
