@@ -408,6 +408,8 @@ __device__ __forceinline__ void mic_r(const MicRegs& m, float& dx, float& dy, fl
 // same on any IEEE machine with an FMA (the CPU check reproduces it bit for
 // bit).  Max error 0.501 ulp over normal inputs; inputs outside [2^-120, 2^120]
 // (zero, denormals, inf, NaN) take the correctly rounded reciprocal.
+__device__ __noinline__ float rcp_rare(float x) { return __frcp_rn(x); }
+
 __device__ __forceinline__ float rcp_nr(float x) {
   float y = __int_as_float(0x7EF311C3 - __float_as_int(x));
 #pragma unroll
@@ -415,7 +417,9 @@ __device__ __forceinline__ float rcp_nr(float x) {
     const float e = __fmaf_rn(-x, y, 1.0f);
     y = __fmaf_rn(y, e, y);
   }
-  if (!(x >= 0x1p-120f && x <= 0x1p120f)) y = __frcp_rn(x);  // rare
+  // rare: a branch to an out-of-line call keeps the correctly rounded
+  // reciprocal's instructions off the common path
+  if (__builtin_expect(!(x >= 0x1p-120f && x <= 0x1p120f), 0)) y = rcp_rare(x);
   return y;
 }
 
