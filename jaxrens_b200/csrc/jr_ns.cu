@@ -179,7 +179,7 @@ __device__ __forceinline__ void walk_chain(const JrParams& P, Walker<G>& w, int 
   for (int t0 = 0; t0 < T; t0 += kStepChunk) {
     const int nt = T - t0 < kStepChunk ? T - t0 : kStepChunk;
     for (int q = w.g.rank(); q < nt; q += w.g.size()) {
-      s.step_key[q] = split(chain_key, (uint32_t)(t0 + q));
+      s.step_key[q] = make_step_key(split(chain_key, (uint32_t)(t0 + q)));
       s.step_move[q] = choice(split(move_key, (uint32_t)(t0 + q)), P.moves.cum_probs,
                               P.moves.n_moves);
     }
@@ -782,7 +782,8 @@ move_trial_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st, co
     idx = choice(mk, P.moves.cum_probs, P.moves.n_moves);
   }
   int reason = 0;
-  const bool acc = gated_move<true>(P, w, idx, key, step[p], emax[p], st.pressure[p], mu, reason);
+  const bool acc = gated_move<true>(P, w, idx, make_step_key(key), step[p], emax[p], st.pressure[p],
+                                   mu, reason);
   w.g.sync();
   if (w.g.leader()) {
     accepted[tb] = acc ? 1 : 0;

@@ -21,6 +21,16 @@ namespace jr {
 
 constexpr int kMaxWarps = 32;
 constexpr int kStepChunk = 64;  // steps whose keys and moves are drawn at once
+
+// The key of one MWG step with its two first-level subkeys, split(k, 0) and
+// split(k, 1), which every move draws from (galilean: initial direction and
+// perturbation; volume and cell moves: proposal and prior; identity moves:
+// atom and species).
+struct StepKey {
+  Key k, k0, k1;
+};
+
+__device__ __forceinline__ StepKey make_step_key(Key k) { return StepKey{k, split(k, 0u), split(k, 1u)}; }
 constexpr int kPairMatMax = 96;  // walkers up to this size use the pair matrix
                                  // (12 n pm_stride(n) bytes: 112 KB at 96; measured faster than
                                  // the ordered pairs from 32 to 96 atoms)
@@ -119,7 +129,7 @@ struct WalkShared {
   int c_nev[JR_MAX_MOVES];
   int c_ngr[JR_MAX_MOVES];
   // step keys and move choices of the next steps of a chain
-  Key step_key[kStepChunk];
+  StepKey step_key[kStepChunk];
   int step_move[kStepChunk];
   int cell_ok;  // cell-geometry verdict of the pending cell move
   // pre-move copy for the constraint gate
@@ -881,12 +891,12 @@ __device__ __forceinline__ double galilean_trajectory(const JrParams& P, Walker<
 // reflection d - 2 (f.d) f with f = F/|F| is evaluated as
 // d - [2 (F.d) / max(|F|,1e-10)^2] F from two float64 sums.
 template <class G>
-__device__ __forceinline__ bool move_galilean(const JrParams& P, Walker<G>& w, Key key, float step, int R,
+__device__ __forceinline__ bool move_galilean(const JrParams& P, Walker<G>& w, const StepKey& key, float step, int R,
                               float pa, double emax, float pressure, const float* mu) {
   const WalkArrays& arr = w.arr;
   const int n3 = 3 * w.n;
   const int r0 = w.g.rank(), gs = w.g.size();
-  const Key ki = split(key, 0u), kp = split(key, 1u);
+  const Key ki = key.k0, kp = key.k1;
   // |d|^2 and |d + pa * normal|^2 in one group reduction; a direction of
   // norm < 1e-8 (a walker's first galilean move) then redraws a fresh normal
   // direction and reduces its norm separately.  The sums are the ones of
@@ -985,14 +995,14 @@ __device__ inline bool cell_valid(const float* c, int n, const JrMoveParams& mv)
 // Volume move (volume.py:49-109 + _common.py:16-93).  Returns acceptance and
 // the reject reason (priority energy > cell > prior).
 template <class G>
-__device__ __forceinline__ bool move_volume(const JrParams& P, Walker<G>& w, Key key, float step, double emax,
+__device__ __forceinline__ bool move_volume(const JrParams& P, Walker<G>& w, const StepKey& key, float step, double emax,
                             float pressure, const float* mu, int& reason) {
   WalkShared& s = w.s;
   const WalkArrays& arr = w.arr;
   const int n = w.n;
   const int r0 = w.g.rank(), gs = w.g.size();
   const JrMoveParams& mv = P.moves;
-  const Key k1 = split(key, 0u), k2 = split(key, 1u);
+  const Key k1 = key.k0, k2 = key.k1;
   const int cur = s.cur, tr = cur ^ 1;
   const float* h = s.cc[cur].raw;
   const float oldV = s.cc[cur].vol;
@@ -1110,10 +1120,10 @@ __device__ __forceinline__ float norm3_f(const float* v) {
 // rv1 v1n + rv2 v2n within the plane of the other two rows, (rv1, rv2) =
 // step * normal(k2, (2,)); T = solve(old, new) in float64.
 template <class G>
-__device__ __forceinline__ bool move_shear(const JrParams& P, Walker<G>& w, Key key, float step,
+__device__ __forceinline__ bool move_shear(const JrParams& P, Walker<G>& w, const StepKey& key, float step,
                                            double emax, float pressure, const float* mu,
                                            int& reason) {
-  const Key k1 = split(key, 0u), k2 = split(key, 1u);
+  const Key k1 = key.k0, k2 = key.k1;
   const int a = randint(k1, 0, 3);
   const float rv1 = __fmul_rn(step, normal(bits32(k2, 0u)));
   const float rv2 = __fmul_rn(step, normal(bits32(k2, 1u)));
@@ -1163,10 +1173,10 @@ __device__ __forceinline__ bool move_shear(const JrParams& P, Walker<G>& w, Key 
 // [randint(k1, 0, 3)], rv = step * normal(k2); T = diag with exp(rv) at i
 // and exp(-rv) at j (float64 exp rounded to float32); cell . T, x . T.
 template <class G>
-__device__ __forceinline__ bool move_stretch(const JrParams& P, Walker<G>& w, Key key,
+__device__ __forceinline__ bool move_stretch(const JrParams& P, Walker<G>& w, const StepKey& key,
                                              float step, double emax, float pressure,
                                              const float* mu, int& reason) {
-  const Key k1 = split(key, 0u), k2 = split(key, 1u);
+  const Key k1 = key.k0, k2 = key.k1;
   const int pr = randint(k1, 0, 3);
   const int ai = pr == 2 ? 1 : 0, aj = pr == 0 ? 1 : 2;
   const float rv = __fmul_rn(step, normal(bits32(k2, 0u)));
@@ -1184,13 +1194,13 @@ __device__ __forceinline__ bool move_stretch(const JrParams& P, Walker<G>& w, Ke
 
 // alchemical_morph (alchemical.py:40-79).
 template <class G>
-__device__ __forceinline__ bool move_morph(const JrParams& P, Walker<G>& w, Key key, double emax,
+__device__ __forceinline__ bool move_morph(const JrParams& P, Walker<G>& w, const StepKey& key, double emax,
                            float pressure, const float* mu) {
   WalkShared& s = w.s;
   const WalkArrays& arr = w.arr;
-  const int atom = randint(split(key, 0u), 0, w.n);
+  const int atom = randint(key.k0, 0, w.n);
   const int curt = __float_as_int(arr.xs[atom].w);
-  const int cand = randint(split(key, 1u), 0, P.model.n_species - 1);
+  const int cand = randint(key.k1, 0, P.model.n_species - 1);
   const int nt = cand + (cand >= curt ? 1 : 0);
   w.g.sync();
   if (w.g.leader()) {
@@ -1218,14 +1228,14 @@ __device__ __forceinline__ bool move_morph(const JrParams& P, Walker<G>& w, Key 
 
 // species_swap over all species (swap.py:177-260).
 template <class G>
-__device__ __forceinline__ bool move_swap(const JrParams& P, Walker<G>& w, Key key, double emax, float pressure,
+__device__ __forceinline__ bool move_swap(const JrParams& P, Walker<G>& w, const StepKey& key, double emax, float pressure,
                           const float* mu) {
   constexpr int kMaxPairs = JR_MAX_SPECIES * (JR_MAX_SPECIES - 1) / 2;
   WalkShared& s = w.s;
   const WalkArrays& arr = w.arr;
   const int n = w.n;
   const int S = P.model.n_species;
-  const Key kp = split(key, 0u), klo = split(key, 1u), khi = split(key, 2u);
+  const Key kp = key.k0, klo = key.k1, khi = split(key.k, 2u);
   int counts[JR_MAX_SPECIES];
   for (int q = 0; q < S; ++q) counts[q] = s.counts[q];
   uint8_t plo[kMaxPairs], phi[kMaxPairs];
@@ -1286,7 +1296,7 @@ __device__ __forceinline__ bool move_swap(const JrParams& P, Walker<G>& w, Key k
 
 // One move of type P.moves.type[idx]; returns acceptance and reject reason.
 template <class G>
-__device__ __forceinline__ bool run_move(const JrParams& P, Walker<G>& w, int idx, Key key,
+__device__ __forceinline__ bool run_move(const JrParams& P, Walker<G>& w, int idx, const StepKey& key,
                                          float step, double emax, float pressure,
                                          const float* mu, int& reason) {
   reason = 0;
@@ -1361,7 +1371,7 @@ __device__ inline bool min_distance_ok(const JrParams& P, Walker<G>& w) {
 // gated and no shear/stretch move is present: the extra code, inlined into
 // the walk loop, was measured to slow every chain by about 9%.
 template <bool kExt, class G>
-__device__ __forceinline__ bool gated_move(const JrParams& P, Walker<G>& w, int idx, Key key,
+__device__ __forceinline__ bool gated_move(const JrParams& P, Walker<G>& w, int idx, const StepKey& key,
                                            float step, double emax, float pressure,
                                            const float* mu, int& reason) {
   if constexpr (!kExt) {
@@ -1406,7 +1416,7 @@ __device__ __forceinline__ bool gated_move(const JrParams& P, Walker<G>& w, int 
 // MWG step (mwg.py:227-257 with the _wrap counters of mwg.py:108-150) plus
 // the ns_step scan-body counters (nested_sampling.py:541-609).
 template <bool kExt, class G>
-__device__ __forceinline__ void mwg_step(const JrParams& P, Walker<G>& w, Key step_key, int idx,
+__device__ __forceinline__ void mwg_step(const JrParams& P, Walker<G>& w, const StepKey& step_key, int idx,
                                          double emax, float pressure, const float* mu) {
   WalkShared& s = w.s;
   int reason = 0;
