@@ -179,11 +179,30 @@ __device__ __forceinline__ void walk_chain(const JrParams& P, Walker<G>& w, int 
   for (int t0 = 0; t0 < T; t0 += kStepChunk) {
     const int nt = T - t0 < kStepChunk ? T - t0 : kStepChunk;
     for (int q = w.g.rank(); q < nt; q += w.g.size()) {
-      s.step_key[q] = make_step_key(split(chain_key, (uint32_t)(t0 + q)));
-      s.step_move[q] = choice(split(move_key, (uint32_t)(t0 + q)), P.moves.cum_probs,
-                              P.moves.n_moves);
+      StepKey sk = make_step_key(split(chain_key, (uint32_t)(t0 + q)));
+      const int mi = choice(split(move_key, (uint32_t)(t0 + q)), P.moves.cum_probs,
+                            P.moves.n_moves);
+      const int ty = P.moves.type[mi];
+      if (ty == JR_MOVE_VOLUME) {
+        sk.vn = normal(bits32(sk.k0, 0u));
+        sk.vu = uniform01(bits32(sk.k1, 0u));
+        sk.pre = 1;
+      } else if (ty == JR_MOVE_GALILEAN && w.arr.nz) {
+        sk.nz = w.arr.nz + (size_t)q * 3 * w.n;
+      }
+      s.step_key[q] = sk;
+      s.step_move[q] = mi;
     }
     w.g.sync();
+    // the galilean perturbation normals of the chunk, all threads at once
+    if (w.arr.nz) {
+      const int n3 = 3 * w.n;
+      for (int e = w.g.rank(); e < nt * n3; e += w.g.size()) {
+        const int t = e / n3, q = e - t * n3;
+        if (s.step_key[t].nz) w.arr.nz[e] = normal(bits32(s.step_key[t].k1, (uint32_t)q));
+      }
+      w.g.sync();
+    }
     for (int t = 0; t < nt; ++t)
       mwg_step<kExt>(P, w, s.step_key[t], s.step_move[t], emax, pressure, mu);
     w.g.sync();
@@ -255,7 +274,7 @@ __device__ inline DynLayout dyn_layout(unsigned char* dyn, int K, int nmax, int 
   L.pij = use_pair_matrix(nmax, nimg) ? reinterpret_cast<uint16_t*>(p) : nullptr;
   p += pair_table_bytes(nmax, nimg);
   L.walkers = p;
-  L.walker_bytes = walker_smem_bytes(nmax, nimg);
+  L.walker_bytes = walker_smem_bytes(nmax, nimg, true);
   return L;
 }
 
@@ -510,7 +529,7 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
   DynLayout L = dyn_layout(dyn, K, D.n_atoms_max, nimg, D.n_cull);
   WalkArrays arr;
   WalkShared* wsp = carve_walker(L.walkers + (size_t)my * L.walker_bytes, D.n_atoms_max, nimg,
-                                 L.pij, arr);
+                                 L.pij, arr, true);
   Walker<G> w{*wsp, arr, tab, n, tpa, make_group<G>(red), 0};
   zero_pair_matrix(w.g, arr, D.n_atoms_max);
   int par = 0;
@@ -1180,7 +1199,7 @@ int check_config(const JrLaunchConfig& c, const JrDims* d) {
 size_t ns_dyn_smem(const JrDims* d, const JrParams* p, const JrLaunchConfig& c) {
   const int cpc = c.warp_walkers ? c.threads / 32 : 1;
   return jr::dyn_head_bytes(d->n_walkers, d->n_atoms_max, p->model.n_images, d->n_cull) +
-         (size_t)cpc * jr::walker_smem_bytes(d->n_atoms_max, p->model.n_images);
+         (size_t)cpc * jr::walker_smem_bytes(d->n_atoms_max, p->model.n_images, true);
 }
 
 size_t group_dyn_smem(int nmax, int nimg, int groups) {

@@ -28,9 +28,22 @@ constexpr int kStepChunk = 64;  // steps whose keys and moves are drawn at once
 // atom and species).
 struct StepKey {
   Key k, k0, k1;
+  // draws of the step made ahead of the walk (they depend on the keys only):
+  // nz, when set, holds the galilean perturbation normals normal(bits(k1, q));
+  // with pre set, vn = normal(bits(k0, 0)) and vu = uniform(bits(k1, 0)) of a
+  // volume step
+  const float* nz;
+  float vn, vu;
+  int pre;
 };
 
-__device__ __forceinline__ StepKey make_step_key(Key k) { return StepKey{k, split(k, 0u), split(k, 1u)}; }
+__device__ __forceinline__ StepKey make_step_key(Key k) {
+  return StepKey{k, split(k, 0u), split(k, 1u), nullptr, 0.0f, 0.0f, 0};
+}
+
+// The largest walker (atoms) whose NS chains get a buffer for the galilean
+// normals of a chunk of steps (kStepChunk x 3 n floats).
+constexpr int kNormalAtomsMax = 32;
 constexpr int kPairMatMax = 96;  // walkers up to this size use the pair matrix
                                  // (12 n pm_stride(n) bytes: 112 KB at 96; measured faster than
                                  // the ordered pairs from 32 to 96 atoms)
@@ -160,6 +173,7 @@ struct WalkArrays {
   float* T;             // [2][3 n_img] image translations for cc[0], cc[1]
   float* pm;            // [3][n][pm_stride(n)] pair force terms g*dr_ij, or nullptr
   const uint16_t* pij;  // [Nmax(Nmax-1)/2] pair decode a | b << 8, or nullptr
+  float* nz;            // [kStepChunk][3 n] galilean normals drawn ahead, or nullptr
 };
 
 __host__ __device__ inline bool use_pair_matrix(int nmax, int nimg) {
@@ -180,12 +194,18 @@ __host__ __device__ inline size_t pair_count(int nmax) {
   return (size_t)nmax * (size_t)(nmax - 1) / 2;
 }
 
-// Bytes of one walker: WalkShared + arrays (+ pair buffer).
-__host__ __device__ inline size_t walker_smem_bytes(int nmax, int nimg) {
+// Bytes of one walker: WalkShared + arrays (+ pair buffer) (+ the buffer of
+// normals drawn ahead, for the NS chains of small walkers).
+__host__ __device__ inline bool use_normal_buffer(int nmax, bool normals) {
+  return normals && nmax <= kNormalAtomsMax;
+}
+
+__host__ __device__ inline size_t walker_smem_bytes(int nmax, int nimg, bool normals = false) {
   size_t b = align16(sizeof(WalkShared));
   b += 2u * 16u * (size_t)nmax + 4u * 12u * (size_t)nmax;
   b += align16(2u * 3u * 4u * (size_t)nimg);
   if (use_pair_matrix(nmax, nimg)) b += align16(12u * (size_t)nmax * (size_t)pm_stride(nmax));
+  if (use_normal_buffer(nmax, normals)) b += align16(12u * (size_t)kStepChunk * (size_t)nmax);
   return align16(b);
 }
 
@@ -195,7 +215,7 @@ __host__ __device__ inline size_t pair_table_bytes(int nmax, int nimg) {
 }
 
 __device__ inline WalkShared* carve_walker(char* p, int nmax, int nimg, const uint16_t* pij,
-                                           WalkArrays& a) {
+                                           WalkArrays& a, bool normals = false) {
   WalkShared* s = reinterpret_cast<WalkShared*>(p);
   p += align16(sizeof(WalkShared));
   a.xs = (float4*)p; p += 16 * nmax;
@@ -208,10 +228,12 @@ __device__ inline WalkShared* carve_walker(char* p, int nmax, int nimg, const ui
   if (use_pair_matrix(nmax, nimg)) {
     a.pm = (float*)p;
     a.pij = pij;
+    p += align16(12u * (size_t)nmax * (size_t)pm_stride(nmax));
   } else {
     a.pm = nullptr;
     a.pij = nullptr;
   }
+  a.nz = use_normal_buffer(nmax, normals) ? (float*)p : nullptr;
   return s;
 }
 
@@ -904,7 +926,8 @@ __device__ __forceinline__ bool move_galilean(const JrParams& P, Walker<G>& w, c
   double sq = 0.0, sv = 0.0, zero = 0.0;
   for (int q = r0; q < n3; q += gs) {
     const float d = arr.dir[q];
-    const float v = __fmaf_rn(pa, normal(bits32(kp, (uint32_t)q)), d);
+    const float g = key.nz ? key.nz[q] : normal(bits32(kp, (uint32_t)q));
+    const float v = __fmaf_rn(pa, g, d);
     sq += (double)d * (double)d;
     sv += (double)v * (double)v;
     arr.dir[q] = v;
@@ -1007,7 +1030,7 @@ __device__ __forceinline__ bool move_volume(const JrParams& P, Walker<G>& w, con
   const float* h = s.cc[cur].raw;
   const float oldV = s.cc[cur].vol;
   const float sn = __fmul_rn(step, (float)n);
-  const float dV = __fmul_rn(sn, normal(bits32(k1, 0u)));
+  const float dV = __fmul_rn(sn, key.pre ? key.vn : normal(bits32(k1, 0u)));
   const float newV = fabsf(__fadd_rn(oldV, dV));
   const float ratio = __fdiv_rn(newV, oldV);
   const float scale = __double2float_rn(pow((double)ratio, (double)(1.0f / 3.0f)));
@@ -1028,7 +1051,7 @@ __device__ __forceinline__ bool move_volume(const JrParams& P, Walker<G>& w, con
   double d0, d1;
   const double En = ham_eval<false>(P, w, tr, pressure, mu, d0, d1);
   const bool valid = s.cell_ok != 0;
-  const float u = uniform01(bits32(k2, 0u));
+  const float u = key.pre ? key.vu : uniform01(bits32(k2, 0u));
   bool prior_ok;
   if (mv.flat_v_prior) {
     prior_ok = u < 1.0f;
