@@ -5,6 +5,10 @@
 * LJ8 NPT: an ensemble of GPU runs and an ensemble of runs of the oracle in
   the reference's float32 arithmetic (independent seeds) give the same log Z
   and the same heat-capacity peak temperature within statistical error.
+* LJ-32 NPT at the bench shape (8 runs x 512 walkers, n_mcmc_steps 40, 10
+  reflections): GPU and oracle ensembles give the same log Z after 6000
+  iterations (prior mass about 1e-5), so the throughput is measured at
+  matched log Z.
 """
 
 import numpy as np
@@ -82,3 +86,39 @@ def test_lj8_npt_log_z_and_cv_peak_match_reference_arithmetic():
     tr = np.array([_cv_peak(dead_r[r], live_r[r], K, N) for r in range(P)])
     se_t = np.sqrt(tg.var(ddof=1) / P + tr.var(ddof=1) / P)
     assert abs(tg.mean() - tr.mean()) < 4 * se_t + 0.03, (tg, tr)
+
+
+def test_lj32_npt_bench_shape_log_z_matches_reference_arithmetic():
+    """Matched log Z at the bench shape: 8 runs x 512 walkers of 32-atom LJ
+    NPT at one pressure (so the runs form one seed ensemble), n_mcmc_steps 40,
+    10 reflections, 6000 iterations (prior mass exp(-6000/512), about 1e-5).
+    The GPU ensemble and an independent ensemble of oracle runs in the
+    reference's float32 arithmetic give the same log Z (dead points plus live
+    walkers) and the same final contour within statistical error."""
+    P, K, N, T, n_iter = 8, 512, 32, 40, 6000
+    la = prior_mass.log_alpha(K, 1)
+    wo = float(prior_mass.iteration_offsets(K, 1)[1][0])
+    gcase = lj_case(P=P, K=K, N=N, seed=300, n_reflect=10, T=T, pressure=0.1)
+    ns = nsm.init_ns_parallel(gcase["init_fn"], gcase["positions"], gcase["types"],
+                              gcase["energies"], gcase["cells"], gcase["run_keys"],
+                              ensemble_params={"pressure": gcase["pressures"]})
+    dead_g, live_g = _run_gpu(ns, gcase["step"], n_iter, T)
+    rcase = lj_case(P=P, K=K, N=N, seed=400, n_reflect=10, T=T, pressure=0.1)
+    reps = oracle_replicas(rcase)
+    dead_r = np.zeros((P, n_iter))
+    for it in range(n_iter):
+        infos = O.ns_step_batched(rcase["model"], rcase["moves"], reps, T, la, wo,
+                                  shared_move_key=True, mode=O.REF32, n_threads=8)
+        dead_r[:, it] = [i.dead_energy for i in infos]
+    live_r = np.stack([r.energy for r in reps])
+    lz_g = np.array([thermo.log_evidence(dead_g[r], live_g[r], K) for r in range(P)])
+    lz_r = np.array([thermo.log_evidence(dead_r[r], live_r[r], K) for r in range(P)])
+    se = np.sqrt(lz_g.var(ddof=1) / P + lz_r.var(ddof=1) / P)
+    print("log Z GPU %.4f +- %.4f, oracle %.4f +- %.4f" %
+          (lz_g.mean(), lz_g.std(ddof=1), lz_r.mean(), lz_r.std(ddof=1)))
+    assert abs(lz_g.mean() - lz_r.mean()) < 4 * se + 0.05, (lz_g, lz_r)
+    eg, er = dead_g[:, -1], dead_r[:, -1]
+    se_e = np.sqrt(eg.var(ddof=1) / P + er.var(ddof=1) / P)
+    print("final contour GPU %.4f +- %.4f, oracle %.4f +- %.4f" %
+          (eg.mean(), eg.std(ddof=1), er.mean(), er.std(ddof=1)))
+    assert abs(eg.mean() - er.mean()) < 4 * se_e + 1e-3 * abs(er.mean()), (eg, er)
