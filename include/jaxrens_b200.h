@@ -67,7 +67,8 @@ enum {
   JR_ERR_UNSUPPORTED = -6  /* a feature the library does not implement */
 };
 
-enum { JR_MODEL_LJ = 0, JR_MODEL_GAUSS_MIX = 1 };
+enum { JR_MODEL_LJ = 0, JR_MODEL_GAUSS_MIX = 1, JR_MODEL_SW = 2 };
+#define JR_SW_MAX_ATOMS 64
 enum { JR_MOVE_GALILEAN = 0, JR_MOVE_VOLUME = 1, JR_MOVE_MORPH = 2,
        JR_MOVE_SWAP = 3, JR_MOVE_SHEAR = 4, JR_MOVE_STRETCH = 5 };
 
@@ -84,9 +85,15 @@ typedef struct JrDims {
 } JrDims;
 
 /* Energy model: LJ with per-species-pair tables (or the Gaussian-mixture
- * validation toy).  Tables are row-major S x S, already in the float32 form
- * the reference evaluates: eps4 = f32(4*eps_ij), eps24 = f32(24*eps_ij),
- * sig2 = f32(sigma_ij**2). */
+ * validation toy, or Stillinger-Weber).  LJ tables are row-major S x S,
+ * already in the float32 form the reference evaluates: eps4 = f32(4*eps_ij),
+ * eps24 = f32(24*eps_ij), sig2 = f32(sigma_ij**2).
+ * JR_MODEL_SW: Stillinger-Weber (Phys. Rev. B 31, 5262 (1985)) with p = 4,
+ * q = 0, one species, n_images = 1, at most JR_SW_MAX_ATOMS atoms; the sw_*
+ * fields hold its float32 constants (sigma, a*sigma, gamma*sigma, A*eps, B,
+ * lambda*eps) and rc2 = f32(sw_rc**2), has_cutoff = 1.  It has no
+ * counterpart in the reference, which plugs potentials in through its
+ * EnergyBackend protocol (src/jaxrens/backends/base.py:165-212). */
 typedef struct JrModelParams {
   int32_t model;
   int32_t n_species;
@@ -100,6 +107,7 @@ typedef struct JrModelParams {
   int32_t n_centers;
   float centers[JR_MAX_CENTERS * 3];
   float gm_sigma;
+  float sw_sigma, sw_rc, sw_gsig, sw_Aeps, sw_B, sw_leps;
 } JrModelParams;
 
 typedef struct JrMoveParams {
@@ -162,6 +170,10 @@ typedef struct JrInfoBuffers {
   int32_t* n_grad_evaluations;     /* [n_iter][P][M] */
   int32_t* rounds;                 /* [P] speculation rounds used (diagnostic) */
   double* dead_energy;             /* [n_iter][P][n_cull] energies of the culled walkers */
+  /* [n_iter][P][4] Stillinger-Weber work of the iteration's chains: pairs and
+   * triplets inside the cutoff summed over the energy+force evaluations, then
+   * over the energy-only ones (zero for the other models) */
+  int64_t* term_counts;
 } JrInfoBuffers;
 
 /* Launch shape of the walk kernels.  threads: CTA size; tpa: threads per
@@ -177,6 +189,9 @@ typedef struct JrLaunchConfig {
 } JrLaunchConfig;
 
 /* ---- NS iterations (replaces the jit'd ns_step) ---- */
+/* Device workspace bytes jr_ns_iterate needs: the snapshot of replica 0's key
+ * words (8 bytes) in one 256-byte slot.  The size does not depend on dims in
+ * this version; callers ask anyway. */
 size_t jr_ns_iterate_workspace_size(const JrDims* dims);
 
 /* Runs n_iter NS iterations on every replica.  `cfg` may be NULL (cached
@@ -194,7 +209,9 @@ int jr_ns_iterate(const JrDims* dims, const JrParams* params,
  * dims whose jr_ns_iterate_workspace_size() exceeds 256 bytes are rejected
  * with JR_ERR_WORKSPACE.  It allocates nothing.  The first call on each
  * device resolves that array's address (cudaGetSymbolAddress, device
- * current) and caches it, so make that first call before any stream capture.
+ * current) and caches it with the id of the device's CUDA context, so make
+ * that first call before any stream capture; after cudaDeviceReset the next
+ * call sees a new context and resolves the address again.
  * The scratch is shared by every call on a device: calls that overlap in
  * time (several host threads, or concurrent streams) race on it and must be
  * serialised by the caller. */

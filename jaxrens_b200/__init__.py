@@ -14,7 +14,9 @@ from .backends import (
     GaussianMixtureBackend,
     Hamiltonian,
     LJBackend,
+    StillingerWeberBackend,
     create_lj,
+    create_sw,
     eval_energy_and_forces,
 )
 from .moves import (MoveKernel, alchemical, galilean, gmc, morph_move, shear, shear_move, stretch,
@@ -41,7 +43,7 @@ from .nested_sampling import (
 
 __all__ = [
     "BackendResult", "EnsembleTerm", "GaussianMixtureBackend", "Hamiltonian", "LJBackend",
-    "create_lj", "eval_energy_and_forces", "MoveKernel", "alchemical", "galilean", "gmc",
+    "StillingerWeberBackend", "create_lj", "create_sw", "eval_energy_and_forces", "MoveKernel", "alchemical", "galilean", "gmc",
     "morph_move", "swap", "swap_move", "volume", "volume_move", "shear", "shear_move",
     "stretch", "stretch_move", "build_mwg",
     "InterREManager", "IterationTermination", "NSState", "PriorMassTermination",

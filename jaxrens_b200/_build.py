@@ -14,17 +14,23 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = os.path.join(HERE, "csrc", "jr_ns.cu")
-DEPS = [
-    os.path.join(HERE, "csrc", f)
-    for f in ("jr_ns.cu", "jr_rng.cuh", "jr_walk.cuh", "jr_tune.cu")
-] + [os.path.join(ROOT, "include", "jaxrens_b200.h")]
+CSRC = os.path.join(HERE, "csrc")
+# translation units linked into the one library (each is self-contained)
+SRCS = [os.path.join(CSRC, f) for f in ("jr_ns.cu", "jr_pair_ext.cu", "jr_pair_aux.cu", "jr_sw.cu")]
+
+
+def _deps() -> list[str]:
+    hdrs = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))
+            if f.endswith((".cu", ".cuh"))]
+    return hdrs + [os.path.join(ROOT, "include", "jaxrens_b200.h")]
+
+
 OUT = os.path.join(HERE, "_lib", "libjaxrens_b200.so")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
 ]
 
 
@@ -32,19 +38,31 @@ def _stale() -> bool:
     if not os.path.exists(OUT):
         return True
     t = os.path.getmtime(OUT)
-    return any(os.path.exists(d) and os.path.getmtime(d) > t for d in DEPS)
+    return any(os.path.getmtime(d) > t for d in _deps())
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every translation unit to an object in parallel, then link."""
     if not force and not _stale():
         return OUT
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    srcs = [SRC] + [p for p in [os.path.join(HERE, "csrc", "jr_tune.cu")] if os.path.exists(p)]
-    cmd = ["nvcc", *NVCC_FLAGS, "-o", OUT + ".tmp", *srcs]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True)
+    objdir = os.path.join(HERE, "_lib", "_obj")
+    os.makedirs(objdir, exist_ok=True)
+    procs, objs = [], []
+    for src in SRCS:
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        cmd = ["nvcc", *NVCC_FLAGS, "-c", "-o", obj, src]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+            print(" ".join(cmd), file=sys.stderr)
+        procs.append((subprocess.Popen(cmd), cmd))
+        objs.append(obj)
+    failed = [cmd for p, cmd in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
+    link = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+            "-Xcompiler", "-fPIC", "-o", OUT + ".tmp", *objs]
+    subprocess.run(link, check=True)
     os.replace(OUT + ".tmp", OUT)
     return OUT
 

@@ -26,7 +26,8 @@ ERRORS = {
     -6: "JR_ERR_UNSUPPORTED",
 }
 
-MODEL_LJ, MODEL_GAUSS_MIX = 0, 1
+MODEL_LJ, MODEL_GAUSS_MIX, MODEL_SW = 0, 1, 2
+SW_MAX_ATOMS = 64
 MOVE_GALILEAN, MOVE_VOLUME, MOVE_MORPH, MOVE_SWAP, MOVE_SHEAR, MOVE_STRETCH = 0, 1, 2, 3, 4, 5
 
 _vp = C.c_void_p
@@ -59,6 +60,12 @@ class JrModelParams(C.Structure):
         ("n_centers", C.c_int32),
         ("centers", C.c_float * (MAX_CENTERS * 3)),
         ("gm_sigma", C.c_float),
+        ("sw_sigma", C.c_float),
+        ("sw_rc", C.c_float),
+        ("sw_gsig", C.c_float),
+        ("sw_Aeps", C.c_float),
+        ("sw_B", C.c_float),
+        ("sw_leps", C.c_float),
     ]
 
 
@@ -124,6 +131,7 @@ class JrInfoBuffers(C.Structure):
         ("n_grad_evaluations", _vp),
         ("rounds", _vp),
         ("dead_energy", _vp),
+        ("term_counts", _vp),
     ]
 
 

@@ -56,15 +56,17 @@ class LJBackend:
         sig = np.asarray(sigma, np.float32)
         if eps.ndim != sig.ndim:
             raise ValueError(
-                "epsilon and sigma must have the same rank, got "
-                f"epsilon.ndim={eps.ndim}, sigma.ndim={sig.ndim}")
+                f"epsilon (rank {eps.ndim}) and sigma (rank {sig.ndim}) differ in rank; "
+                "pass two scalars, two per-species vectors or two pair tables")
         if eps.ndim > 2:
-            raise ValueError(f"epsilon/sigma must be scalar, 1-D or 2-D, got rank {eps.ndim}")
+            raise ValueError(f"rank-{eps.ndim} epsilon/sigma: only scalars, per-species "
+                             "vectors and S x S pair tables are accepted")
         if eps.ndim >= 1 and eps.shape != sig.shape:
             raise ValueError(
-                f"per-species epsilon and sigma must have matching length, got {eps.shape} vs {sig.shape}")
+                f"epsilon has shape {eps.shape} but sigma has shape {sig.shape}; "
+                "give both one entry per species")
         if eps.ndim >= 1 and eps.shape[0] == 0:
-            raise ValueError("per-species epsilon/sigma must be non-empty")
+            raise ValueError("empty epsilon/sigma tables: a species table needs at least one entry")
         if eps.ndim == 2 and (eps.shape[0] != eps.shape[1] or not np.array_equal(eps, eps.T)
                               or not np.array_equal(sig, sig.T)):
             raise ValueError("pair tables must be square and symmetric")
@@ -167,6 +169,71 @@ class GaussianMixtureBackend:
     def energy_and_forces(self, positions, species, cell, max_neighbors=0,
                           ensemble_params=None):
         return _evaluate(self, None, positions, species, cell, forces=True)
+
+
+class StillingerWeberBackend:
+    """Stillinger-Weber potential (F. H. Stillinger and T. A. Weber, Phys.
+    Rev. B 31, 5262 (1985)) for one species with the exponents p = 4, q = 0:
+    two-body ``A eps (B (sigma/r)^4 - 1) exp(sigma / (r - a sigma))`` and
+    three-body ``lambda eps (cos theta + 1/3)^2 g(r_ij) g(r_ik)``,
+    ``g(r) = exp(gamma sigma / (r - a sigma))``, zero beyond ``a sigma``,
+    under the single minimum image.
+
+    The reference has no such backend; it takes one through its
+    ``EnergyBackend`` protocol (``backends/base.py:165-212``), which this
+    class follows (``__call__``, ``energy_and_forces``, ``r_cutoff``).
+    Defaults are the silicon parameters (eV, Angstrom).
+    """
+
+    def __init__(self, epsilon: float = 2.1683, sigma: float = 2.0951, a: float = 1.8,
+                 lambda_: float = 21.0, gamma: float = 1.2, A: float = 7.049556277,
+                 B: float = 0.6022245584, p: int = 4, q: int = 0):
+        if int(p) != 4 or int(q) != 0:
+            raise NotImplementedError(
+                f"the Stillinger-Weber kernels take the exponents p = 4, q = 0 (got p={p}, q={q})")
+        if min(epsilon, sigma, a) <= 0.0:
+            raise ValueError("epsilon, sigma and a must be positive")
+        self.epsilon, self.sigma, self.a = float(epsilon), float(sigma), float(a)
+        self.lambda_, self.gamma, self.A, self.B = float(lambda_), float(gamma), float(A), float(B)
+        self.n_species = 1
+        self.cutoff = self.a * self.sigma
+        self.r_cutoff = self.cutoff
+        f = np.float32
+        # the float32 constants of the kernel contract, rounded once here
+        self.consts = dict(sw_sigma=f(sigma), sw_rc=f(self.a * self.sigma),
+                           sw_gsig=f(self.gamma * self.sigma), sw_Aeps=f(self.A * self.epsilon),
+                           sw_B=f(self.B), sw_leps=f(self.lambda_ * self.epsilon))
+
+    def model_params(self) -> _lib.JrModelParams:
+        m = _lib.JrModelParams()
+        m.model = _lib.MODEL_SW
+        m.n_species = 1
+        m.has_cutoff = 1
+        rc = self.consts["sw_rc"]
+        m.rc2 = float(np.float32(rc * rc))
+        m.n_images = 1
+        for k, v in self.consts.items():
+            setattr(m, k, float(v))
+        return m
+
+    def __call__(self, positions, species, cell, max_neighbors: int = 0,
+                 ensemble_params: dict | None = None) -> BackendResult:
+        return _evaluate(self, None, positions, species, cell, forces=False)
+
+    def energy_and_forces(self, positions, species, cell, max_neighbors: int = 0,
+                          ensemble_params: dict | None = None) -> BackendResult:
+        return _evaluate(self, None, positions, species, cell, forces=True)
+
+
+def create_sw(epsilon: float = 2.1683, sigma: float = 2.0951, a: float = 1.8,
+              lambda_: float = 21.0, gamma: float = 1.2, A: float = 7.049556277,
+              B: float = 0.6022245584, p: int = 4, q: int = 0) -> StillingerWeberBackend:
+    return StillingerWeberBackend(epsilon=epsilon, sigma=sigma, a=a, lambda_=lambda_,
+                                  gamma=gamma, A=A, B=B, p=p, q=q)
+
+
+#: eV / Angstrom^3 per GPa (pressures of the Stillinger-Weber workloads)
+EV_PER_A3_PER_GPA = 0.006241509
 
 
 class EnergyTerm:

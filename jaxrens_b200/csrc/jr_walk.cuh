@@ -22,6 +22,14 @@ namespace jr {
 constexpr int kMaxWarps = 32;
 constexpr int kStepChunk = 64;  // steps whose keys and moves are drawn at once
 
+// Model families, fixed at compile time per kernel instantiation (carried by
+// the group type): the pair family (LJ and the Gaussian-mixture toy) and the
+// Stillinger-Weber family.  A kernel of one family compiles no code of the
+// other, so each family's walk keeps its own registers and instruction
+// stream.
+constexpr int kFamPair = 0;
+constexpr int kFamSW = 1;
+
 // The key of one MWG step with its two first-level subkeys, split(k, 0) and
 // split(k, 1), which every move draws from (galilean: initial direction and
 // perturbation; volume and cell moves: proposal and prior; identity moves:
@@ -44,6 +52,7 @@ __device__ __forceinline__ StepKey make_step_key(Key k) {
 // The largest walker (atoms) whose NS chains get a buffer for the galilean
 // normals of a chunk of steps (kStepChunk x 3 n floats).
 constexpr int kNormalAtomsMax = 32;
+constexpr int kSWMaxAtoms = 64;  // Stillinger-Weber walkers: one 64-bit neighbour mask per atom
 constexpr int kPairMatMax = 96;  // walkers up to this size use the pair matrix
                                  // (12 n pm_stride(n) bytes: 112 KB at 96; measured faster than
                                  // the ordered pairs from 32 to 96 atoms)
@@ -52,7 +61,10 @@ constexpr int kPairMatMax = 96;  // walkers up to this size use the pair matrix
 
 // A whole CTA walking one walker.  sum3 reduces three doubles across the
 // block through two alternating shared buffers (one barrier per reduction).
-struct CtaGroup {
+template <int kFamily>
+struct CtaG {
+  static constexpr int kFam = kFamily;
+  static constexpr bool kIsWarp = false;
   double (*red)[kMaxWarps][3];  // smem [2][kMaxWarps][3]
   __device__ __forceinline__ int rank() const { return threadIdx.x; }
   __device__ __forceinline__ int size() const { return blockDim.x; }
@@ -93,7 +105,10 @@ struct CtaGroup {
 };
 
 // One warp walking one walker: register shuffles only, no block barriers.
-struct WarpGroup {
+template <int kFamily>
+struct WarpG {
+  static constexpr int kFam = kFamily;
+  static constexpr bool kIsWarp = true;
   __device__ __forceinline__ int rank() const { return threadIdx.x & 31; }
   __device__ __forceinline__ int size() const { return 32; }
   __device__ __forceinline__ void sync() const { __syncwarp(); }
@@ -113,6 +128,9 @@ struct WarpGroup {
     (void)par;
   }
 };
+
+using CtaGroup = CtaG<kFamPair>;
+using WarpGroup = WarpG<kFamPair>;
 
 // ----------------------------------------------------------- walker ----
 
@@ -145,6 +163,11 @@ struct WalkShared {
   StepKey step_key[kStepChunk];
   int step_move[kStepChunk];
   int cell_ok;  // cell-geometry verdict of the pending cell move
+  int sw_nitems;  // Stillinger-Weber: neighbour pairs of the current evaluation
+  // Stillinger-Weber: pairs and triplets inside the cutoff summed over the
+  // chain's evaluations, [energy+forces pairs, triplets, energy-only pairs,
+  // triplets] (the algorithmic work of the chain)
+  long long c_terms[4];
   // pre-move copy for the constraint gate
   double E_save;
   int cur_save;
@@ -174,10 +197,17 @@ struct WalkArrays {
   float* pm;            // [3][n][pm_stride(n)] pair force terms g*dr_ij, or nullptr
   const uint16_t* pij;  // [Nmax(Nmax-1)/2] pair decode a | b << 8, or nullptr
   float* nz;            // [kStepChunk][3 n] galilean normals drawn ahead, or nullptr
+  // Stillinger-Weber tables (the SW family only), one record per unordered
+  // pair of the row-major upper triangle:
+  float4* swr0;         // [n(n-1)/2] (dr, 1/r) of pairs inside the cutoff
+  float4* swr1;         // [n(n-1)/2] (g, g'/(g r), phi2'/r, phi2)
+  float4* swq;          // [n(n-1)/2] pair force share Q_ab
+  uint64_t* nbm;        // [2][kSWMaxAtoms] neighbour masks (alternating evaluations)
+  uint16_t* items;      // [n(n-1)/2] neighbour pairs a | b << 8
 };
 
-__host__ __device__ inline bool use_pair_matrix(int nmax, int nimg) {
-  return nimg == 1 && nmax <= kPairMatMax;
+__host__ __device__ inline bool use_pair_matrix(int nmax, int nimg, int fam = kFamPair) {
+  return fam == kFamPair && nimg == 1 && nmax <= kPairMatMax;
 }
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
@@ -200,22 +230,32 @@ __host__ __device__ inline bool use_normal_buffer(int nmax, bool normals) {
   return normals && nmax <= kNormalAtomsMax;
 }
 
-__host__ __device__ inline size_t walker_smem_bytes(int nmax, int nimg, bool normals = false) {
+// Bytes of the Stillinger-Weber tables of one walker.
+__host__ __device__ inline size_t sw_table_bytes(int nmax) {
+  const size_t np = pair_count(nmax);
+  return 3u * 16u * np + 2u * 8u * (size_t)kSWMaxAtoms + align16(2u * np);
+}
+
+__host__ __device__ inline size_t walker_smem_bytes(int nmax, int nimg, bool normals = false,
+                                                    int fam = kFamPair) {
   size_t b = align16(sizeof(WalkShared));
   b += 2u * 16u * (size_t)nmax + 4u * 12u * (size_t)nmax;
   b += align16(2u * 3u * 4u * (size_t)nimg);
-  if (use_pair_matrix(nmax, nimg)) b += align16(12u * (size_t)nmax * (size_t)pm_stride(nmax));
+  if (use_pair_matrix(nmax, nimg, fam)) b += align16(12u * (size_t)nmax * (size_t)pm_stride(nmax));
+  if (fam == kFamSW) b += sw_table_bytes(nmax);
   if (use_normal_buffer(nmax, normals)) b += align16(12u * (size_t)kStepChunk * (size_t)nmax);
   return align16(b);
 }
 
-// Bytes of the CTA-shared pair decode table.
-__host__ __device__ inline size_t pair_table_bytes(int nmax, int nimg) {
-  return use_pair_matrix(nmax, nimg) ? align16(2u * pair_count(nmax)) : 0;
+// Bytes of the CTA-shared pair decode table (the pair-matrix path and every
+// Stillinger-Weber walk).
+__host__ __device__ inline size_t pair_table_bytes(int nmax, int nimg, int fam = kFamPair) {
+  return (use_pair_matrix(nmax, nimg, fam) || fam == kFamSW) ? align16(2u * pair_count(nmax)) : 0;
 }
 
 __device__ inline WalkShared* carve_walker(char* p, int nmax, int nimg, const uint16_t* pij,
-                                           WalkArrays& a, bool normals = false) {
+                                           WalkArrays& a, bool normals = false,
+                                           int fam = kFamPair) {
   WalkShared* s = reinterpret_cast<WalkShared*>(p);
   p += align16(sizeof(WalkShared));
   a.xs = (float4*)p; p += 16 * nmax;
@@ -225,13 +265,24 @@ __device__ inline WalkShared* carve_walker(char* p, int nmax, int nimg, const ui
   a.dp = (float*)p; p += 12 * nmax;
   a.F = (float*)p; p += 12 * nmax;
   a.T = (float*)p; p += align16(2 * 3 * 4 * nimg);
-  if (use_pair_matrix(nmax, nimg)) {
+  a.pm = nullptr;
+  a.pij = nullptr;
+  a.swr0 = a.swr1 = a.swq = nullptr;
+  a.nbm = nullptr;
+  a.items = nullptr;
+  if (use_pair_matrix(nmax, nimg, fam)) {
     a.pm = (float*)p;
     a.pij = pij;
     p += align16(12u * (size_t)nmax * (size_t)pm_stride(nmax));
-  } else {
-    a.pm = nullptr;
-    a.pij = nullptr;
+  }
+  if (fam == kFamSW) {
+    const size_t np = pair_count(nmax);
+    a.pij = pij;
+    a.swr0 = (float4*)p; p += 16u * np;
+    a.swr1 = (float4*)p; p += 16u * np;
+    a.swq = (float4*)p; p += 16u * np;
+    a.nbm = (uint64_t*)p; p += 2u * 8u * kSWMaxAtoms;
+    a.items = (uint16_t*)p; p += align16(2u * np);
   }
   a.nz = use_normal_buffer(nmax, normals) ? (float*)p : nullptr;
   return s;
@@ -241,6 +292,8 @@ __device__ inline WalkShared* carve_walker(char* p, int nmax, int nimg, const ui
 // group synchronises before the first evaluation.
 template <class G>
 __device__ inline void zero_pair_matrix(const G& g, const WalkArrays& a, int nmax) {
+  if (a.nbm != nullptr)
+    for (int q = g.rank(); q < 2 * kSWMaxAtoms; q += g.size()) a.nbm[q] = 0ull;
   if (a.pm == nullptr) return;
   const int words = 3 * nmax * pm_stride(nmax);
   for (int q = g.rank(); q < words; q += g.size()) a.pm[q] = 0.0f;
@@ -272,6 +325,7 @@ struct Walker {
   int tpa;
   G g;
   int par;
+  int swpar = 0;  // Stillinger-Weber: which neighbour-mask buffer the next evaluation uses
 };
 
 __device__ __forceinline__ float& pos_at(float4* xs, int idx) {
@@ -440,7 +494,7 @@ __device__ __forceinline__ void mic_r(const MicRegs& m, float& dx, float& dy, fl
 // same on any IEEE machine with an FMA (the CPU check reproduces it bit for
 // bit).  Max error 0.501 ulp over normal inputs; inputs outside [2^-120, 2^120]
 // (zero, denormals, inf, NaN) take the correctly rounded reciprocal.
-__device__ __noinline__ float rcp_rare(float x) { return __frcp_rn(x); }
+__device__ __noinline__ inline float rcp_rare(float x) { return __frcp_rn(x); }
 
 __device__ __forceinline__ float rcp_nr(float x) {
   float y = __int_as_float(0x7EF311C3 - __float_as_int(x));
@@ -779,11 +833,16 @@ __device__ __forceinline__ void pairs_ordered(const JrParams& P, Walker<G>& w, c
   sfd = fd_part;
 }
 
-// Model energy U (forces into arr.F when kForces) of the walker; also sum(F^2)
-// and sum(F . dir) for the galilean reflection.  Results are group-uniform.
+}  // namespace jr
+
+#include "jr_sw.cuh"
+
+namespace jr {
+
+// The pair family's models: the Gaussian-mixture toy and LJ.
 template <bool kForces, class G>
-__device__ __forceinline__ void model_eval(const JrParams& P, Walker<G>& w, int cidx, double& U, double& sff,
-                           double& sfd) {
+__device__ __forceinline__ void model_eval_pair(const JrParams& P, Walker<G>& w, int cidx,
+                                                double& U, double& sff, double& sfd) {
   const WalkArrays& arr = w.arr;
   const JrModelParams& mp = P.model;
   if (mp.model == JR_MODEL_GAUSS_MIX) {
@@ -831,6 +890,20 @@ __device__ __forceinline__ void model_eval(const JrParams& P, Walker<G>& w, int 
   }
 }
 
+// Model energy U (forces into arr.F when kForces) of the walker; also sum(F^2)
+// and sum(F . dir) for the galilean reflection.  Results are group-uniform.
+template <bool kForces, class G>
+__device__ __forceinline__ void model_eval(const JrParams& P, Walker<G>& w, int cidx, double& U, double& sff,
+                           double& sfd) {
+  if constexpr (G::kFam == kFamSW) {
+    const CellCtx& ccs = w.s.cc[cidx];
+    if (ccs.diag) sw_eval<kForces, true>(P, w, load_mic<true>(ccs), U, sff, sfd);
+    else sw_eval<kForces, false>(P, w, load_mic<false>(ccs), U, sff, sfd);
+  } else {
+    model_eval_pair<kForces>(P, w, cidx, U, sff, sfd);
+  }
+}
+
 // Full potential of the walker for cell context cidx: U + (P*V - mu*N).
 template <bool kForces, class G>
 __device__ __forceinline__ double ham_eval(const JrParams& P, Walker<G>& w, int cidx,
@@ -857,7 +930,7 @@ __device__ __forceinline__ double group_sum1(Walker<G>& w, double v) {
 // starts directly on the pair loop; ens is the fixed P V - mu N share.
 // Returns the final potential (NaN read as +inf); the direction is reflected
 // off the contour in place.
-constexpr int kTrajModel = 0, kTrajMatrix = 1, kTrajOrdered = 2;
+constexpr int kTrajModel = 0, kTrajMatrix = 1, kTrajOrdered = 2, kTrajSW = 3;
 
 template <int kPath, bool kS1, bool kDiag, class G>
 __device__ __forceinline__ double galilean_trajectory(const JrParams& P, Walker<G>& w, float step,
@@ -886,7 +959,10 @@ __device__ __forceinline__ double galilean_trajectory(const JrParams& P, Walker<
     }
     w.g.sync();
     double U, sff, sfd;
-    if (kPath == kTrajMatrix) {
+    if constexpr (kPath == kTrajSW) {
+      sw_eval<true, kDiag>(P, w, cc, U, sff, sfd);
+      E = U + ens;
+    } else if (kPath == kTrajMatrix) {
       pairs_matrix<true, kS1, kDiag>(P, w, cc, U, sff, sfd);
       E = U + ens;
     } else if (kPath == kTrajOrdered) {
@@ -953,7 +1029,11 @@ __device__ __forceinline__ bool move_galilean(const JrParams& P, Walker<G>& w, c
   const double E0 = w.s.E;
   double E;
   const JrModelParams& mp = P.model;
-  if (mp.model == JR_MODEL_GAUSS_MIX) {
+  if constexpr (G::kFam == kFamSW) {
+    const double ens = ensemble_term(w.s, w.s.cc[w.s.cur].vol, pressure, mu, mp.n_species);
+    if (w.s.cc[w.s.cur].diag) E = galilean_trajectory<kTrajSW, true, true>(P, w, step, R, emax, ens);
+    else E = galilean_trajectory<kTrajSW, true, false>(P, w, step, R, emax, ens);
+  } else if (mp.model == JR_MODEL_GAUSS_MIX) {
     E = galilean_trajectory<kTrajModel, true, true>(P, w, step, R, emax, 0.0);
   } else {
     // the cell, the species counts and so P V - mu N are fixed for the move
@@ -1546,6 +1626,7 @@ __device__ __forceinline__ void store_walker(const JrDims& D, const JrStateBuffe
 }
 
 __device__ inline void zero_chain_counters(WalkShared& s) {
+  for (int q = 0; q < 4; ++q) s.c_terms[q] = 0;
   for (int m = 0; m < JR_MAX_MOVES; ++m) {
     s.c_acc[m] = s.c_prop[m] = s.c_nev[m] = s.c_ngr[m] = 0;
     s.c_rr[4 * m] = s.c_rr[4 * m + 1] = s.c_rr[4 * m + 2] = s.c_rr[4 * m + 3] = 0;

@@ -286,6 +286,9 @@ class InfoBuffers:
         self.n_evaluations = z((n_iter, P, M), torch.int32)
         self.n_grad_evaluations = z((n_iter, P, M), torch.int32)
         self.rounds = z((P,), torch.int32)
+        # Stillinger-Weber work per iteration: pairs and triplets inside the
+        # cutoff over the energy+force evaluations, then the energy-only ones
+        self.term_counts = z((n_iter, P, 4), torch.int64)
 
     def cstruct(self) -> _lib.JrInfoBuffers:
         b = _lib.JrInfoBuffers()

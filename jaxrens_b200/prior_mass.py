@@ -13,9 +13,10 @@ import numpy as np
 
 def _check(n_live: int, n_cull: int) -> None:
     if int(n_cull) < 1:
-        raise ValueError(f"n_cull must be >= 1, got {n_cull}")
+        raise ValueError(f"at least one walker is culled per iteration (n_cull={n_cull})")
     if int(n_cull) >= int(n_live):
-        raise ValueError(f"n_cull={n_cull} must be smaller than n_live={n_live}")
+        raise ValueError(f"cannot cull {n_cull} of {n_live} live walkers per iteration: "
+                         "n_cull has to stay below n_live")
 
 
 def _terms(n_terms: int, n_live: int, n_cull: int) -> np.ndarray:

@@ -504,6 +504,289 @@ static double lj_f64(const JroModel* m, int n, const float* x,
   return 0.5 * E;
 }
 
+/* ------------------------------------------------------------------ */
+/* Stillinger-Weber (Phys. Rev. B 31, 5262 (1985)), p = 4, q = 0        */
+/* ------------------------------------------------------------------ */
+
+/* exp(x) of the kernel contract: Cody-Waite reduction x = k ln2 + r with
+ * k = rint(x log2 e), ln2 = LN2_HI + LN2_LO (LN2_HI: float32 ln2 with its 12
+ * low mantissa bits cleared), the degree-7 Taylor polynomial of e^r (1/n! in
+ * float32) in FMA Horner form, scaled by 2^k (two steps below the normal
+ * range). */
+float jro_sw_exp(float x) {
+  if (!(x > -104.0f)) return 0.0f;
+  if (x > 88.5f) return INFINITY;
+  const float k = rintf(x * 0x1.715476p+0f);
+  float r = fmaf(-k, 0x1.62ep-1f, x);
+  r = fmaf(-k, 0x1.0bfbe8p-15f, r);
+  float p = 0x1.a01a02p-13f;
+  p = fmaf(p, r, 0x1.6c16c2p-10f);
+  p = fmaf(p, r, 0x1.111112p-7f);
+  p = fmaf(p, r, 0x1.555556p-5f);
+  p = fmaf(p, r, 0x1.555556p-3f);
+  p = fmaf(p, r, 0.5f);
+  p = fmaf(p, r, 1.0f);
+  p = fmaf(p, r, 1.0f);
+  const int ki = (int)k;
+  uint32_t b;
+  float sc;
+  if (ki >= -126) {
+    b = (uint32_t)(ki + 127) << 23;
+    memcpy(&sc, &b, 4);
+    return p * sc;
+  }
+  b = (uint32_t)(ki + 64 + 127) << 23;
+  memcpy(&sc, &b, 4);
+  return (p * sc) * 0x1p-64f;
+}
+
+typedef struct SwPair {
+  float dx, dy, dz, inv_r, g, u, c2, e2;
+} SwPair;
+
+static inline int sw_pidx(int lo, int hi, int n) { return lo * (2 * n - lo - 1) / 2 + (hi - lo - 1); }
+
+/* The kernel's pair record (float32, the kernel's op order). */
+static int sw_pair_dev(const JroModel* m, float r2, SwPair* q) {
+  if (!(r2 < m->rc2)) return 0;
+  const float r = sqrtf(r2);
+  if (!(r < m->sw_rc)) return 0;
+  q->inv_r = rcp_nr(r);
+  const float md = m->sw_rc - r;
+  const float inv_md = rcp_nr(md);
+  const float ex = jro_sw_exp(-(m->sw_sigma * inv_md));
+  q->g = jro_sw_exp(-(m->sw_gsig * inv_md));
+  const float sg = m->sw_sigma * q->inv_r;
+  const float s2 = sg * sg;
+  const float s4 = s2 * s2;
+  const float bq = fmaf(m->sw_B, s4, -1.0f);
+  const float aex = m->sw_Aeps * ex;
+  q->e2 = aex * bq;
+  const float w = (m->sw_sigma * inv_md) * inv_md;
+  const float t1 = (-4.0f * (m->sw_B * s4)) * q->inv_r;
+  const float dphi = aex * fmaf(-bq, w, t1);
+  q->c2 = dphi * q->inv_r;
+  q->u = (-((m->sw_gsig * inv_md) * inv_md)) * q->inv_r;
+  return 1;
+}
+
+/* One triplet seen from leg j (other leg k): force on j subtracted from v,
+ * energy returned (the kernel's sw_triplet). */
+static float sw_triplet_dev(float leps, const float* jv, float ij, float gj, float uj,
+                            const float* kv, float ik, float gk, float* v, int forces) {
+  const float dot = fmaf(jv[2], kv[2], fmaf(jv[1], kv[1], jv[0] * kv[0]));
+  const float cs = (dot * ij) * ik;
+  const float t = cs + 0x1.555556p-2f;
+  const float G = (leps * gj) * gk;
+  const float tG = t * G;
+  if (forces) {
+    const float ij2 = ij * ij;
+    const float p2 = (2.0f * cs) * ij2;
+    const float A = tG * fmaf(t, uj, -p2);
+    const float Bc = (2.0f * tG) * (ij * ik);
+    for (int q = 0; q < 3; ++q) v[q] = v[q] - fmaf(A, jv[q], Bc * kv[q]);
+  }
+  return tG * t;
+}
+
+/* The kernel contract (DEV): pair records, per neighbour pair {a<b} the two
+ * centre sides with the other leg ascending, Q_ab = c2 dr_ab + V_ba - V_ab,
+ * F_i gathered over neighbours in blocks of 8 then the pairwise tree.  Also
+ * used for REF32: the reference has no Stillinger-Weber to take an op order
+ * from.  *n_pairs / *n_trip receive the evaluation's counts (may be NULL). */
+static double sw_dev(const JroModel* m, int n, const float* x, const float* cell_in, double* F,
+                     int64_t* n_pairs, int64_t* n_trip) {
+  float safe[9];
+  const float* c = cell_in;
+  if (jro_det3(cell_in) == 0.0f) {
+    memset(safe, 0, sizeof(safe));
+    safe[0] = safe[4] = safe[8] = 1.0e10f;
+    c = safe;
+  }
+  float inv[9];
+  jro_inv_cell(c, inv);
+  const int np = n * (n - 1) / 2;
+  SwPair* pr = (SwPair*)calloc((size_t)(np > 0 ? np : 1), sizeof(SwPair));
+  float* Q = (float*)calloc((size_t)(np > 0 ? np : 1) * 3, sizeof(float));
+  uint64_t nbm[64];
+  memset(nbm, 0, sizeof(nbm));
+  double E = 0.0;
+  for (int a = 0; a < n; ++a)
+    for (int b = a + 1; b < n; ++b) {
+      float dr[3], d[3], nn[3];
+      for (int q = 0; q < 3; ++q) dr[q] = x[3 * b + q] - x[3 * a + q];
+      for (int q = 0; q < 3; ++q) {
+        float f = dr[0] * inv[q];
+        f = fmaf(dr[1], inv[3 + q], f);
+        f = fmaf(dr[2], inv[6 + q], f);
+        nn[q] = rintf(f);
+      }
+      for (int q = 0; q < 3; ++q) {
+        float sv = nn[0] * c[q];
+        sv = fmaf(nn[1], c[3 + q], sv);
+        sv = fmaf(nn[2], c[6 + q], sv);
+        d[q] = dr[q] - sv;
+      }
+      float r2 = d[0] * d[0];
+      r2 = fmaf(d[1], d[1], r2);
+      r2 = fmaf(d[2], d[2], r2);
+      SwPair* q = pr + sw_pidx(a, b, n);
+      if (sw_pair_dev(m, r2, q)) {
+        q->dx = d[0];
+        q->dy = d[1];
+        q->dz = d[2];
+        nbm[a] |= 1ull << b;
+        nbm[b] |= 1ull << a;
+        E += (double)q->e2;
+      }
+    }
+  int64_t pairs = 0, trip = 0;
+  for (int i = 0; i < n; ++i) {
+    const int dg = __builtin_popcountll(nbm[i]);
+    pairs += dg;
+    trip += dg * (dg - 1) / 2;
+  }
+  if (n_pairs) *n_pairs = pairs / 2;
+  if (n_trip) *n_trip = trip;
+  for (int a = 0; a < n; ++a)
+    for (int b = a + 1; b < n; ++b) {
+      if (!((nbm[a] >> b) & 1ull)) continue;
+      const int p = sw_pidx(a, b, n);
+      const SwPair* ab = pr + p;
+      float vab[3] = {0.0f, 0.0f, 0.0f}, vba[3] = {0.0f, 0.0f, 0.0f};
+      for (int side = 0; side < 2; ++side) {
+        const int ctr = side == 0 ? a : b, leg = side == 0 ? b : a;
+        const float sg = side == 0 ? 1.0f : -1.0f;
+        const float jv[3] = {sg * ab->dx, sg * ab->dy, sg * ab->dz};
+        float* v = side == 0 ? vab : vba;
+        for (int k = 0; k < n; ++k) {
+          if (k == leg || !((nbm[ctr] >> k) & 1ull)) continue;
+          const int fwd = ctr < k;
+          const SwPair* ck = pr + (fwd ? sw_pidx(ctr, k, n) : sw_pidx(k, ctr, n));
+          const float kv[3] = {fwd ? ck->dx : -ck->dx, fwd ? ck->dy : -ck->dy,
+                               fwd ? ck->dz : -ck->dz};
+          if (F || k > leg) {
+            const float h = sw_triplet_dev(m->sw_leps, jv, ab->inv_r, ab->g, ab->u, kv,
+                                           ck->inv_r, ck->g, v, F != NULL);
+            if (k > leg) E += (double)h;
+          }
+        }
+      }
+      if (F) {
+        const float dv[3] = {ab->dx, ab->dy, ab->dz};
+        for (int q = 0; q < 3; ++q) Q[3 * p + q] = fmaf(ab->c2, dv[q], vba[q]) - vab[q];
+      }
+    }
+  if (F) {
+    int nb = (n + 7) / 8, L = 1;
+    while (L < nb) L <<= 1;
+    for (int i = 0; i < n; ++i) {
+      float Pb[32][3];
+      memset(Pb, 0, sizeof(Pb));
+      for (int bk = 0; bk < L; ++bk) {
+        const int j0 = 8 * bk, j1 = j0 + 8 < n ? j0 + 8 : n;
+        for (int j = j0; j < j1; ++j) {
+          if (!((nbm[i] >> j) & 1ull)) continue;
+          const int fwd = i < j;
+          const float* qv = Q + 3 * (fwd ? sw_pidx(i, j, n) : sw_pidx(j, i, n));
+          for (int q = 0; q < 3; ++q) Pb[bk][q] = Pb[bk][q] + (fwd ? qv[q] : -qv[q]);
+        }
+      }
+      for (int st = 1; st < L; st <<= 1) {
+        float T2[32][3];
+        for (int bk = 0; bk < L; ++bk)
+          for (int q = 0; q < 3; ++q) T2[bk][q] = Pb[bk][q] + Pb[bk ^ st][q];
+        memcpy(Pb, T2, sizeof(float) * 3 * L);
+      }
+      for (int q = 0; q < 3; ++q) F[3 * i + q] = (double)Pb[0][q];
+    }
+  }
+  free(pr);
+  free(Q);
+  return E;
+}
+
+/* Everything in double, written independently of the kernel's organisation:
+ * pair sum over i < j, triplet sum over centres i and leg pairs j < k, forces
+ * from the analytic gradient of each term added to the three atoms. */
+static double sw_f64(const JroModel* m, int n, const float* x, const float* cell_in, double* F) {
+  double c[9], inv[9];
+  for (int i = 0; i < 9; ++i) c[i] = (double)cell_in[i];
+  if (jro_det3(cell_in) == 0.0f) {
+    memset(c, 0, sizeof(c));
+    c[0] = c[4] = c[8] = 1.0e10;
+  }
+  inv_cell_f64(c, inv);
+  const double sig = m->sw_sigma, rc = m->sw_rc, gsig = m->sw_gsig, Ae = m->sw_Aeps,
+               B = m->sw_B, le = m->sw_leps;
+  double* D = (double*)calloc((size_t)n * n * 3, sizeof(double));  /* MIC dr_ij = x_j - x_i */
+  double* R = (double*)calloc((size_t)n * n, sizeof(double));
+  if (F) memset(F, 0, sizeof(double) * 3 * (size_t)n);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      if (i == j) continue;
+      double dr[3], nn[3];
+      for (int q = 0; q < 3; ++q) dr[q] = (double)x[3 * j + q] - (double)x[3 * i + q];
+      for (int q = 0; q < 3; ++q)
+        nn[q] = nearbyint(dr[0] * inv[q] + dr[1] * inv[3 + q] + dr[2] * inv[6 + q]);
+      for (int q = 0; q < 3; ++q)
+        D[3 * (i * n + j) + q] = dr[q] - (nn[0] * c[q] + nn[1] * c[3 + q] + nn[2] * c[6 + q]);
+      const double* d = D + 3 * (i * n + j);
+      R[i * n + j] = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    }
+  double E = 0.0;
+  for (int i = 0; i < n; ++i)
+    for (int j = i + 1; j < n; ++j) {
+      const double r = R[i * n + j];
+      if (!(r < rc)) continue;
+      const double s4 = pow(sig / r, 4.0);
+      const double ex = exp(sig / (r - rc));
+      E += Ae * (B * s4 - 1.0) * ex;
+      if (F) {
+        const double dphi = Ae * ex * (-4.0 * B * s4 / r - (B * s4 - 1.0) * sig / ((r - rc) * (r - rc)));
+        const double* d = D + 3 * (i * n + j);
+        for (int q = 0; q < 3; ++q) {
+          F[3 * i + q] += dphi * d[q] / r;
+          F[3 * j + q] -= dphi * d[q] / r;
+        }
+      }
+    }
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      if (j == i || !(R[i * n + j] < rc)) continue;
+      for (int k = j + 1; k < n; ++k) {
+        if (k == i || !(R[i * n + k] < rc)) continue;
+        const double* dj = D + 3 * (i * n + j);
+        const double* dk = D + 3 * (i * n + k);
+        const double rj = R[i * n + j], rk = R[i * n + k];
+        const double cs = (dj[0] * dk[0] + dj[1] * dk[1] + dj[2] * dk[2]) / (rj * rk);
+        const double gj = exp(gsig / (rj - rc)), gk = exp(gsig / (rk - rc));
+        const double t = cs + 1.0 / 3.0;
+        E += le * t * t * gj * gk;
+        if (F) {
+          /* dh/dx_j = le gj gk [t^2 g'j/gj drj/rj + 2t dcos/dx_j] */
+          const double lj = -gsig / ((rj - rc) * (rj - rc)), lk = -gsig / ((rk - rc) * (rk - rc));
+          const double G = le * gj * gk;
+          double hj[3], hk[3];
+          for (int q = 0; q < 3; ++q) {
+            const double dcj = dk[q] / (rj * rk) - cs * dj[q] / (rj * rj);
+            const double dck = dj[q] / (rj * rk) - cs * dk[q] / (rk * rk);
+            hj[q] = G * (t * t * lj * dj[q] / rj + 2.0 * t * dcj);
+            hk[q] = G * (t * t * lk * dk[q] / rk + 2.0 * t * dck);
+          }
+          for (int q = 0; q < 3; ++q) {
+            F[3 * j + q] -= hj[q];
+            F[3 * k + q] -= hk[q];
+            F[3 * i + q] += hj[q] + hk[q];
+          }
+        }
+      }
+    }
+  free(D);
+  free(R);
+  return E;
+}
+
 /* Gaussian-mixture toy (backends/toy.py:163-204), evaluated in double. */
 static double gauss_mix(const JroModel* m, int n, const float* x, double* F) {
   double com[3] = {0, 0, 0};
@@ -547,6 +830,9 @@ double jro_energy(const JroModel* mdl, int32_t mode, int32_t n, const float* x,
   double U;
   if (mdl->model == JRO_MODEL_GAUSS_MIX) {
     U = gauss_mix(mdl, n, x, forces);
+  } else if (mdl->model == JRO_MODEL_SW) {
+    U = mode == JRO_F64 ? sw_f64(mdl, n, x, cell, forces)
+                        : sw_dev(mdl, n, x, cell, forces, NULL, NULL);
   } else if (mode == JRO_DEV) {
     U = lj_dev(mdl, n, x, types, cell, forces);
   } else if (mode == JRO_REF32) {

@@ -10,6 +10,10 @@
  *     `jax_threefry_partitionable=True` layout,
  *   - the LJ backend (src/jaxrens/backends/lj.py:125-204) with per-species
  *     tables, triclinic minimum image, supercell images and a hard cutoff,
+ *   - the Stillinger-Weber potential (Phys. Rev. B 31, 5262 (1985); no
+ *     counterpart in the reference, which plugs such backends in through
+ *     src/jaxrens/backends/base.py:165-212) -- parity unpinned against any
+ *     external implementation, pinned by its closed forms instead,
  *   - the EnsembleTerm P*V - mu*N (src/jaxrens/backends/ensemble.py:34-59),
  *   - the galilean / volume / alchemical-morph / species-swap moves
  *     (the files under src/jaxrens/sampling/moves/), the MWG step
@@ -38,7 +42,7 @@ extern "C" {
 enum { JRO_DEV = 0, JRO_REF32 = 1, JRO_F64 = 2 };
 enum { JRO_MOVE_GALILEAN = 0, JRO_MOVE_VOLUME = 1, JRO_MOVE_MORPH = 2,
        JRO_MOVE_SWAP = 3, JRO_MOVE_SHEAR = 4, JRO_MOVE_STRETCH = 5 };
-enum { JRO_MODEL_LJ = 0, JRO_MODEL_GAUSS_MIX = 1 };
+enum { JRO_MODEL_LJ = 0, JRO_MODEL_GAUSS_MIX = 1, JRO_MODEL_SW = 2 };
 
 #define JRO_MAX_SPECIES 8
 #define JRO_MAX_MOVES 8
@@ -59,6 +63,9 @@ typedef struct JroModel {
   int32_t n_centers;
   float centers[JRO_MAX_CENTERS * 3];
   float gm_sigma;
+  /* Stillinger-Weber (p = 4, q = 0, one species): float32 sigma, a*sigma,
+   * gamma*sigma, A*eps, B, lambda*eps; rc2 = float32(sw_rc**2) */
+  float sw_sigma, sw_rc, sw_gsig, sw_Aeps, sw_B, sw_leps;
 } JroModel;
 
 typedef struct JroMoves {
@@ -120,6 +127,10 @@ int32_t jro_randint(const uint32_t key[2], int32_t lo, int32_t hi);
 int32_t jro_choice(const uint32_t key[2], const float* cum, int32_t m);
 void jro_normal_array(const uint32_t key[2], int32_t n, float* out);
 void jro_uniform_array(const uint32_t key[2], int32_t n, float* out);
+
+/* Float32 exp of the Stillinger-Weber kernel contract (Cody-Waite reduction,
+ * degree-7 Taylor polynomial), exposed to test its error bound. */
+float jro_sw_exp(float x);
 
 /* ---- geometry ---- */
 float jro_det3(const float* c);

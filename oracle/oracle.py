@@ -23,7 +23,7 @@ _LIB_PATH = os.path.join(_HERE, "_build", "libjr_oracle.so")
 
 DEV, REF32, F64 = 0, 1, 2
 GALILEAN, VOLUME, MORPH, SWAP = 0, 1, 2, 3
-MODEL_LJ, MODEL_GAUSS_MIX = 0, 1
+MODEL_LJ, MODEL_GAUSS_MIX, MODEL_SW = 0, 1, 2
 MAX_SPECIES, MAX_MOVES, MAX_IMAGES, MAX_CENTERS = 8, 8, 125, 8
 
 _f = C.POINTER(C.c_float)
@@ -46,6 +46,12 @@ class JroModel(C.Structure):
         ("n_centers", C.c_int32),
         ("centers", C.c_float * (MAX_CENTERS * 3)),
         ("gm_sigma", C.c_float),
+        ("sw_sigma", C.c_float),
+        ("sw_rc", C.c_float),
+        ("sw_gsig", C.c_float),
+        ("sw_Aeps", C.c_float),
+        ("sw_B", C.c_float),
+        ("sw_leps", C.c_float),
     ]
 
 
@@ -124,6 +130,8 @@ def lib():
         L.jro_normal.argtypes = [C.c_uint32]
         L.jro_erfinv.restype = C.c_float
         L.jro_erfinv.argtypes = [C.c_float]
+        L.jro_sw_exp.restype = C.c_float
+        L.jro_sw_exp.argtypes = [C.c_float]
         L.jro_randint.restype = C.c_int32
         L.jro_choice.restype = C.c_int32
         L.jro_det3.restype = C.c_float
@@ -262,6 +270,25 @@ def make_model(eps4, eps24, sig2, rc2=None, img_off=None, model=MODEL_LJ,
         m.centers[: c.size] = c.reshape(-1).tolist()
         m.gm_sigma = np.float32(gm_sigma)
     return m
+
+
+def make_sw_model(sw_sigma, sw_rc, sw_gsig, sw_Aeps, sw_B, sw_leps) -> JroModel:
+    """Stillinger-Weber model from the float32 constants of the kernel
+    contract (one species, the single minimum image)."""
+    m = JroModel()
+    m.model = MODEL_SW
+    m.n_species = 1
+    m.has_cutoff = 1
+    m.sw_sigma, m.sw_rc, m.sw_gsig = (float(np.float32(v)) for v in (sw_sigma, sw_rc, sw_gsig))
+    m.sw_Aeps, m.sw_B, m.sw_leps = (float(np.float32(v)) for v in (sw_Aeps, sw_B, sw_leps))
+    m.rc2 = np.float32(np.float32(sw_rc) * np.float32(sw_rc))
+    m.n_images = 1
+    return m
+
+
+def sw_exp(x: float) -> float:
+    """The SW kernel's float32 exp, evaluated by the oracle."""
+    return float(lib().jro_sw_exp(float(x)))
 
 
 def make_moves(types, n_reflect, perturb_angle, cum_probs, max_vpa=1e4,

@@ -7,12 +7,14 @@ import numpy as np
 
 from jaxrens_b200 import Hamiltonian, EnsembleTerm, build_mwg, create_lj, init as jinit, prng
 from jaxrens_b200 import moves as mvs
-from jaxrens_b200.backends import GaussianMixtureBackend
+from jaxrens_b200.backends import GaussianMixtureBackend, StillingerWeberBackend
 from oracle import oracle as O
 
 
 def oracle_model(backend) -> O.JroModel:
     m = backend.model if hasattr(backend, "model") else backend
+    if isinstance(m, StillingerWeberBackend):
+        return O.make_sw_model(**m.consts)
     if isinstance(m, GaussianMixtureBackend):
         return O.make_model([[0.0]], [[0.0]], [[0.0]], None, None, O.MODEL_GAUSS_MIX,
                             m.centers, m.sigma)
@@ -34,9 +36,11 @@ def lj_case(P=1, K=32, N=8, seed=0, n_reflect=4, T=5, pressure=0.1, epsilon=1.0,
             sigma=1.0, cutoff=2.5, supercell=(1, 1, 1), v_hi_per_atom=8.0,
             n_atoms_list=None, mu=None, identity=None, step_sizes=(0.1, 0.3),
             min_vpa=1.0, max_vpa=1e4, weights=(4.0, 1.0), d_min=None, d_min_types=False,
-            cell_moves=False):
-    """LJ NPT (or semi-grand with identity moves) case with P runs."""
-    lj = create_lj(epsilon=epsilon, sigma=sigma, cutoff=cutoff, supercell_trafo=supercell)
+            cell_moves=False, backend=None):
+    """LJ NPT (or semi-grand with identity moves) case with P runs; another
+    backend (Stillinger-Weber) in place of LJ when ``backend`` is given."""
+    lj = backend if backend is not None else create_lj(epsilon=epsilon, sigma=sigma,
+                                                       cutoff=cutoff, supercell_trafo=supercell)
     S = lj.n_species
     H = Hamiltonian(lj, [EnsembleTerm(pressure=pressure, chemical_potentials=None)])
     Ns = list(n_atoms_list) if n_atoms_list is not None else [N] * P

@@ -44,9 +44,10 @@ def test_struct_layout_matches_header():
 #include <stddef.h>
 #include "jaxrens_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(JrDims), sizeof(JrModelParams),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(JrDims), sizeof(JrModelParams),
          sizeof(JrMoveParams), sizeof(JrParams), sizeof(JrStateBuffers), sizeof(JrInfoBuffers),
-         sizeof(JrLaunchConfig), offsetof(JrParams, log_alpha), offsetof(JrModelParams, gm_sigma));
+         sizeof(JrLaunchConfig), offsetof(JrParams, log_alpha), offsetof(JrModelParams, gm_sigma),
+         offsetof(JrModelParams, sw_leps), offsetof(JrInfoBuffers, term_counts));
   return 0;
 }
 '''
@@ -60,7 +61,8 @@ int main(void) {
     want = [C.sizeof(_lib.JrDims), C.sizeof(_lib.JrModelParams), C.sizeof(_lib.JrMoveParams),
             C.sizeof(_lib.JrParams), C.sizeof(_lib.JrStateBuffers), C.sizeof(_lib.JrInfoBuffers),
             C.sizeof(_lib.JrLaunchConfig), _lib.JrParams.log_alpha.offset,
-            _lib.JrModelParams.gm_sigma.offset]
+            _lib.JrModelParams.gm_sigma.offset, _lib.JrModelParams.sw_leps.offset,
+            _lib.JrInfoBuffers.term_counts.offset]
     assert got == want
 
 
