@@ -56,10 +56,16 @@ def select_workload(name: str) -> None:
     one 8-atom LJ NPT run (P = 0.1) of 128 walkers, n_mcmc_steps = 20.
     ``uneven``: 16 semi-grand runs of binary LJ (sigma AA/BB/AB 1/0.88/0.8,
     epsilon 1/0.5/1.5, cutoff 2.5) with atom counts drawn from {16, 24, ..., 96}
-    (seeded), Delta-mu signed-log-spaced in [-2, 2], 1024 walkers, species
-    Bernoulli(0.5), galilean + volume + morph + swap, n_mcmc_steps = 40, all runs
-    in one launch.  Neither exchanges replicas; a step is 10 NS iterations."""
+    (threefry-seeded), Delta-mu signed-log-spaced in [-2, 2], 1024 walkers,
+    species Bernoulli(0.5) from a threefry key, galilean + volume + morph +
+    swap, n_mcmc_steps = 40, all runs in one launch.  ``sw``: 4 runs of
+    64-atom Stillinger-Weber silicon NPT at 0.1 GPa, 1024 walkers,
+    n_mcmc_steps = 40, the LJ move mix with its steps scaled by the SW sigma
+    (galilean 0.2 A, volume 2.8 A^3 per atom), uniform gas with V in
+    (0, 8 N 20 A^3].  None of these exchanges replicas; a step is 10 NS
+    iterations."""
     global P_RUNS, K, N, T, PRESSURES, CONFIG, N_LIST, MUS, RE_ON, WORKLOAD
+    global V_PER_ATOM, STEP_SIZES
     WORKLOAD = name
     if name == "batched":
         return
@@ -71,8 +77,11 @@ def select_workload(name: str) -> None:
         desc = ("LJ-8 NPT single run (P=0.1) x 128 walkers, n_mcmc_steps=20, "
                 "galilean(n_reflect=10)+volume")
     elif name == "uneven":
+        from jaxrens_b200 import prng
+
         P_RUNS, K, T = 16, 1024, 40
-        N_LIST = [int(v) for v in np.random.default_rng(96).choice(np.arange(16, 97, 8), 16)]
+        u = prng.uniform(prng.fold_in(prng.key(96), 0), P_RUNS)
+        N_LIST = [int(16 + 8 * np.floor(v * 11)) for v in u]
         N = max(N_LIST)
         PRESSURES = np.full(P_RUNS, 0.1, np.float32)
         dmu = np.concatenate([-np.logspace(np.log10(2.0), -2, 8), np.logspace(-2, np.log10(2.0), 8)])
@@ -80,42 +89,63 @@ def select_workload(name: str) -> None:
         desc = ("binary LJ semi-grand (Kob-Andersen pair tables), 16 runs with N in "
                 "{16..96} x 1024 walkers, Delta-mu in [-2, 2], n_mcmc_steps=40, "
                 "galilean(n_reflect=10)+volume+morph+swap")
+    elif name == "sw":
+        from jaxrens_b200.backends import EV_PER_A3_PER_GPA
+
+        P_RUNS, K, N, T = 4, 1024, 64, 40
+        N_LIST = [N] * P_RUNS
+        PRESSURES = np.full(P_RUNS, 0.1 * EV_PER_A3_PER_GPA, np.float32)
+        V_PER_ATOM = 8.0 * 20.0
+        STEP_SIZES = (0.2, 2.8)
+        desc = ("Stillinger-Weber Si-64 NPT, 4 runs at 0.1 GPa x 1024 walkers, "
+                "n_mcmc_steps=40, galilean(n_reflect=10)+volume")
     else:
         raise SystemExit(f"unknown workload {name}")
     CONFIG = {"workload": desc, "n_runs": P_RUNS, "n_walkers": K,
               "n_atoms": N_LIST if name == "uneven" else N, "n_mcmc_steps": T,
               "n_reflect": R_REFLECT, "re_interval": None, "n_cull": 1, "n_extra": 0,
               "iterations_per_step": RE_INTERVAL}
+
+
+V_PER_ATOM = 8.0           # uniform-gas volume bound per atom
+STEP_SIZES = (0.1, 0.3)    # galilean, volume
 # algorithmic flops per unique pair interaction (triclinic MIC accounting)
 FLOPS_EF, FLOPS_E = 61.0, 48.0
+# Stillinger-Weber, per pair / triplet inside the cutoff: energy+forces 74 and
+# 60, energy only 58 and 12
+SW_FLOPS = (74.0, 60.0, 58.0, 12.0)
 
 
 def build_case(seed: int):
-    from jaxrens_b200 import EnsembleTerm, Hamiltonian, build_mwg, create_lj, prng
+    from jaxrens_b200 import EnsembleTerm, Hamiltonian, build_mwg, create_lj, create_sw, prng
     from jaxrens_b200 import init as jinit
     from jaxrens_b200 import moves as mvs
 
     if WORKLOAD == "uneven":
-        lj = create_lj(epsilon=[[1.0, 1.5], [1.5, 0.5]], sigma=[[1.0, 0.8], [0.8, 0.88]],
-                       cutoff=2.5)
+        model = create_lj(epsilon=[[1.0, 1.5], [1.5, 0.5]], sigma=[[1.0, 0.8], [0.8, 0.88]],
+                          cutoff=2.5)
+    elif WORKLOAD == "sw":
+        model = create_sw()
     else:
-        lj = create_lj(epsilon=1.0, sigma=1.0, cutoff=2.5)
-    H = Hamiltonian(lj, [EnsembleTerm(pressure=0.1)])
-    moves = [mvs.gmc(n_reflect=R_REFLECT, step_size=0.1, weight=4.0),
-             mvs.volume_move(N, step_size=0.3, weight=1.0)]
+        model = create_lj(epsilon=1.0, sigma=1.0, cutoff=2.5)
+    H = Hamiltonian(model, [EnsembleTerm(pressure=float(PRESSURES[0]))])
+    moves = [mvs.gmc(n_reflect=R_REFLECT, step_size=STEP_SIZES[0], weight=4.0),
+             mvs.volume_move(N, step_size=STEP_SIZES[1], weight=1.0)]
     if WORKLOAD == "uneven":
         moves += [mvs.morph_move(2, weight=1.0), mvs.swap_move(2, weight=1.0)]
     init_fn, step, _ = build_mwg(H, moves)
     root = prng.key(seed)
-    keys = prng.split(root, P_RUNS + 2)
+    keys = prng.split(root, P_RUNS + 3)
     pos, cells = [], []
     for r in range(P_RUNS):
-        p_, c_ = jinit.uniform_gas(keys[r], K, N_LIST[r], 8.0 * N_LIST[r])
+        p_, c_ = jinit.uniform_gas(keys[r], K, N_LIST[r], V_PER_ATOM * N_LIST[r])
         pos.append(p_)
         cells.append(c_)
     if WORKLOAD == "uneven":
-        rng = np.random.default_rng(seed)
-        types = [rng.integers(0, 2, size=(K, n)).astype(np.int32) for n in N_LIST]
+        # species Bernoulli(0.5), walker-major, from one threefry key per run
+        tkeys = prng.split(keys[P_RUNS + 2], P_RUNS)
+        types = [prng.bernoulli(tkeys[r], K * n, 0.5).astype(np.int32).reshape(K, n)
+                 for r, n in enumerate(N_LIST)]
     else:
         types = [np.zeros((K, N), np.int32) for _ in range(P_RUNS)]
     run_keys = prng.split(keys[P_RUNS], P_RUNS)
@@ -224,15 +254,6 @@ def job_throughput(world: int, iters: int, total_ms: float) -> tuple[float, floa
     return walker_steps / (total_ms * 1e-3), world * P_RUNS * iters / (total_ms * 1e-3)
 
 
-def algorithmic_flops(info) -> float:
-    """Sum over the launch's committed iterations of eval counts x unique
-    pairs x flops per pair (61 energy+forces, 48 energy-only)."""
-    pairs = np.array([n * (n - 1) / 2.0 for n in N_LIST])
-    ne = info.n_evaluations.sum(dim=(0, 2)).cpu().numpy()  # per run
-    ng = info.n_grad_evaluations.sum(dim=(0, 2)).cpu().numpy()
-    return float(np.sum((ng * FLOPS_EF + (ne - ng) * FLOPS_E) * pairs))
-
-
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -256,7 +277,17 @@ def run_ours(args):
     ns = nsm.init_ns_parallel(init_fn, pos, types, None, cells, run_keys, ensemble_params=pr)
     re = nsm.InterREManager(RE_INTERVAL, 1, re_key)
     cfg = None
+    if args.cluster is not None:
+        cfg = _lib.JrLaunchConfig(args.threads, args.tpa, args.cluster, int(args.warp))
+    # prologue: leave the random-gas start before measuring (untimed)
+    info = nsm.InfoBuffers(ns, step.n_moves, RE_INTERVAL, dead=True)
+    for _ in range(args.prologue // RE_INTERVAL):
+        nsm.ns_iterate(ns, step, RE_INTERVAL, T, 0, info=info, cfg=cfg)
+        if RE_ON:
+            re.apply(ns, step)
+    torch.cuda.synchronize()
     if args.tune:
+        # tuned on the walkers past the prologue, the state the timed steps see
         best = _lib.JrLaunchConfig()
         dims = nsm.make_dims(ns, step, T, 0)
         la = nsm.prior_mass.log_alpha(K, 1)
@@ -266,14 +297,6 @@ def run_ours(args):
                                            C.byref(best), torch.cuda.current_stream().cuda_stream),
                    "jr_autotune")
         cfg = best
-    elif args.cluster is not None:
-        cfg = _lib.JrLaunchConfig(args.threads, args.tpa, args.cluster, int(args.warp))
-    # prologue: leave the random-gas start before measuring (untimed)
-    info = nsm.InfoBuffers(ns, step.n_moves, RE_INTERVAL, dead=True)
-    for _ in range(args.prologue // RE_INTERVAL):
-        nsm.ns_iterate(ns, step, RE_INTERVAL, T, 0, info=info, cfg=cfg)
-        if RE_ON:
-            re.apply(ns, step)
     torch.cuda.synchronize()
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -304,15 +327,23 @@ def run_ours(args):
     # flop total outside the events.
     flops_dev = torch.zeros((), dtype=torch.float64, device=dev)
     pairs_dev = torch.tensor([n * (n - 1) / 2.0 for n in N_LIST], dtype=torch.float64, device=dev)
+    sw_flops_dev = torch.tensor(SW_FLOPS, dtype=torch.float64, device=dev)
+    rounds_dev = torch.zeros((), dtype=torch.float64, device=dev)
     it_start = ns.iteration.clone()
     for k in range(args.steps):
         flush.fill_(float(k))  # evict the (L2-resident) walker state between steps
         evs[k][0].record()
         one_step(ev[k])
         evs[k][1].record()
-        ne = info.n_evaluations.sum(dim=(0, 2), dtype=torch.float64)
-        ng = info.n_grad_evaluations.sum(dim=(0, 2), dtype=torch.float64)
-        flops_dev += ((ng * FLOPS_EF + (ne - ng) * FLOPS_E) * pairs_dev).sum()
+        rounds_dev += info.rounds.sum(dtype=torch.float64)
+        if WORKLOAD == "sw":
+            # pairs and triplets inside the cutoff, counted by the kernel
+            tc = info.term_counts.sum(dim=(0, 1), dtype=torch.float64)
+            flops_dev += (tc * sw_flops_dev).sum()
+        else:
+            ne = info.n_evaluations.sum(dim=(0, 2), dtype=torch.float64)
+            ng = info.n_grad_evaluations.sum(dim=(0, 2), dtype=torch.float64)
+            flops_dev += ((ng * FLOPS_EF + (ne - ng) * FLOPS_E) * pairs_dev).sum()
     torch.cuda.synchronize()
     flops = float(flops_dev.item())
     clk = clocks.stop()
@@ -344,12 +375,15 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 pair terms, f64 accumulation", "data": "synthetic",
-        "config": dict(CONFIG, parallelism=f"replicas x{world} GPUs",
-                       l2="flushed (256 MiB write) between timed steps",
-                       launch=None if cfg is None else {"threads": cfg.threads, "tpa": cfg.tpa,
-                                                         "cluster": cfg.cluster,
-                                                         "warp_walkers": cfg.warp_walkers}),
+        "config": dict(CONFIG),
+        "parallelism": f"replicas x{world} GPUs",
+        "l2": "flushed (256 MiB write) between timed steps",
+        "launch": None if cfg is None else {"threads": cfg.threads, "tpa": cfg.tpa,
+                                            "cluster": cfg.cluster,
+                                            "warp_walkers": cfg.warp_walkers,
+                                            "source": "jr_autotune" if args.tune else "flags"},
         "ns_iters_per_s": ns_iters, "ns_iters_per_s_per_run": ns_iters / (world * P_RUNS),
+        "speculation_rounds_per_launch": float(rounds_dev.item()) / (args.steps * P_RUNS),
         "e2e": e2e,
         "gpu_launches": 2 * args.steps,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -457,16 +491,20 @@ def end_to_end(args, ns, step, re, cfg, torch, nsm):
 
 class ReferenceRun:
     """The reference algorithm on host cores: the CPU oracle in the
-    reference's float32 op order, the 8 runs threaded.  The case is built
-    once; ``iterate(n)`` advances every run by n NS iterations and returns
-    the seconds it took."""
+    reference's float32 op order, the runs threaded, replica exchange every
+    ``RE_INTERVAL`` iterations like the GPU arm.  The case is built once and
+    walked through the same untimed prologue as the GPU arm; ``iterate(n)``
+    advances every run by n NS iterations and returns the seconds it took."""
 
-    def __init__(self, seed: int, threads: int):
+    def __init__(self, seed: int, threads: int, prologue: int):
         from jaxrens_b200 import prior_mass
+        from jaxrens_b200 import nested_sampling as nsm
         from oracle import oracle as O
         from tests._cases import oracle_model, oracle_moves
 
-        H, init_fn, step, pos, cells, types, run_keys, _ = build_case(seed)
+        H, init_fn, step, pos, cells, types, run_keys, re_key = build_case(seed)
+        self.re = nsm.InterREManager(RE_INTERVAL, 1, re_key)
+        self.done = 0
         self.O, self.threads = O, threads
         self.model, self.moves = oracle_model(H), oracle_moves(step)
         self.reps = []
@@ -481,7 +519,7 @@ class ReferenceRun:
                                        pressure=float(PRESSURES[r]), mu=mu))
         self.la = prior_mass.log_alpha(K, 1)
         self.wo = float(prior_mass.iteration_offsets(K, 1)[1][0])
-        self.iterate(5)  # past the random-gas start, untimed
+        self.iterate(prologue)  # past the random-gas start, untimed
 
     def iterate(self, n: int) -> float:
         t0 = time.perf_counter()
@@ -489,6 +527,9 @@ class ReferenceRun:
             self.O.ns_step_batched(self.model, self.moves, self.reps, T, self.la, self.wo,
                                    shared_move_key=True, mode=self.O.REF32,
                                    n_threads=self.threads)
+            self.done += 1
+            if RE_ON and self.done % RE_INTERVAL == 0:
+                self.O.re_step(self.reps, self.re.next_swap_key(), 1, mode=self.O.REF32)
         return time.perf_counter() - t0
 
 
@@ -508,10 +549,11 @@ def host_cpu() -> dict:
 
 def cpu_baseline(args):
     threads = min(os.cpu_count() or 1, P_RUNS)
-    dt = ReferenceRun(args.seed, threads).iterate(args.cpu_iters)
+    dt = ReferenceRun(args.seed, threads, args.prologue).iterate(args.cpu_iters)
     return {"value": P_RUNS * T * args.cpu_iters / dt, "unit": "walker-steps/s",
             "cores": threads, "kind": "port", **host_cpu(),
-            "sample": f"{args.cpu_iters} NS iterations x {P_RUNS} runs (after 5 untimed), "
+            "sample": f"{args.cpu_iters} NS iterations x {P_RUNS} runs (after the same "
+                      f"{args.prologue}-iteration untimed prologue as the GPU arm), "
                       f"{dt:.1f} s, CPU oracle in the reference's float32 op order"}
 
 
@@ -522,7 +564,7 @@ def run_reference(args):
     if rank != 0:
         return
     threads = min(os.cpu_count() or 1, P_RUNS)
-    ref = ReferenceRun(args.seed, threads)
+    ref = ReferenceRun(args.seed, threads, args.prologue)
     per_step = max(1, args.cpu_iters // max(1, args.steps))
     for _ in range(args.warmup):
         ref.iterate(per_step)
@@ -534,7 +576,8 @@ def run_reference(args):
         "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * dt / max(1, args.steps), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": dict(CONFIG, parallelism=f"{threads} host threads over runs"),
+        "config": dict(CONFIG),
+        "parallelism": f"{threads} host threads over runs",
         "cpu_baseline": {"value": value, "unit": "walker-steps/s", "cores": threads,
                          "kind": "port", **host_cpu(),
                          "sample": f"{per_step} NS iterations x {P_RUNS} runs per step, "
@@ -555,18 +598,24 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--prologue", type=int, default=200)
-    ap.add_argument("--cpu-iters", type=int, default=2000)
+    ap.add_argument("--cpu-iters", type=int, default=None,
+                    help="NS iterations of the CPU samples (default: 2000, 200 for sw)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--tune", action="store_true")
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="skip jr_autotune (by default it picks the launch shape once, "
+                         "after the prologue and outside the timed region)")
     ap.add_argument("--cluster", type=int, default=None)
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--tpa", type=int, default=8)
     ap.add_argument("--warp", type=int, default=0)
-    ap.add_argument("--workload", default="batched", choices=["batched", "single", "uneven"],
-                    help="batched (default, the headline line), or the single-run and uneven "
-                         "semi-grand configurations")
+    ap.add_argument("--workload", default="batched",
+                    choices=["batched", "single", "uneven", "sw"],
+                    help="batched (default, the headline line), or the single-run, uneven "
+                         "semi-grand and Stillinger-Weber configurations")
     args = ap.parse_args()
     select_workload(args.workload)
+    if args.cpu_iters is None:
+        args.cpu_iters = {"sw": 200, "uneven": 100}.get(args.workload, 2000)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

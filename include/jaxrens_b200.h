@@ -81,7 +81,10 @@ typedef struct JrDims {
   int32_t n_extra;         /* extra walked survivors per iteration */
   int32_t n_cull;          /* culled walkers per iteration, 1..JR_MAX_CULL */
   int32_t shared_move_key; /* 1: move schedule from fold_in(rng_key[0], 1)
-                              (VmapRuns); 0: from each run's own key */
+                              (VmapRuns); 0: from each run's own key;
+                              2: from the caller's key in state.move_key,
+                              shared by every run (ns_step's move_key
+                              argument; one iteration per call) */
 } JrDims;
 
 /* Energy model: LJ with per-species-pair tables (or the Gaussian-mixture
@@ -149,6 +152,8 @@ typedef struct JrStateBuffers {
   const int32_t* n_atoms;
   const float* pressure;
   const float* mu;      /* NULL when the ensemble has no chemical potentials */
+  const uint32_t* move_key;  /* [2] explicit move-schedule key words (device), read
+                                when dims.shared_move_key == 2, else ignored */
 } JrStateBuffers;
 
 /* Per-iteration outputs of jr_ns_iterate, leading axis n_iter then P; the
@@ -263,7 +268,12 @@ int jr_re_swap(const JrDims* dims, const JrStateBuffers* state,
                int32_t n_species, int32_t* acc_per_pair,
                int32_t* att_per_pair, void* stream);
 
-/* ---- autotuner: times launch shapes on a scratch copy of `state` ---- */
+/* ---- autotuner: times launch shapes on a scratch copy of `state` ----
+ * Every candidate shape walks the same trajectory (restored from a pristine
+ * copy before each sample of 4 launches of n_iter_probe iterations), scored
+ * by the median of 3 samples; the winner is cached for these dims and used by
+ * jr_ns_iterate calls given no launch shape.  The caller's state is not
+ * modified.  No counterpart in the reference (the project-written tuner). */
 int jr_autotune(const JrDims* dims, const JrParams* params,
                 const JrStateBuffers* state, int32_t n_iter_probe,
                 JrLaunchConfig* best, void* stream);

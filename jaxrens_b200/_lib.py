@@ -112,6 +112,7 @@ class JrStateBuffers(C.Structure):
         ("n_atoms", _vp),
         ("pressure", _vp),
         ("mu", _vp),
+        ("move_key", _vp),
     ]
 
 

@@ -203,14 +203,22 @@ class StillingerWeberBackend:
         self.consts = dict(sw_sigma=f(sigma), sw_rc=f(self.a * self.sigma),
                            sw_gsig=f(self.gamma * self.sigma), sw_Aeps=f(self.A * self.epsilon),
                            sw_B=f(self.B), sw_leps=f(self.lambda_ * self.epsilon))
+        # the pair test of the kernels is r^2 < rc2 with rc2 the smallest
+        # float32 whose square root reaches the cutoff: exactly r < a sigma
+        rc = self.consts["sw_rc"]
+        x = np.float32(rc * rc)
+        while np.sqrt(x) >= rc:
+            x = np.nextafter(x, np.float32(0))
+        while np.sqrt(x) < rc:
+            x = np.nextafter(x, np.float32(np.inf))
+        self.rc2 = x
 
     def model_params(self) -> _lib.JrModelParams:
         m = _lib.JrModelParams()
         m.model = _lib.MODEL_SW
         m.n_species = 1
         m.has_cutoff = 1
-        rc = self.consts["sw_rc"]
-        m.rc2 = float(np.float32(rc * rc))
+        m.rc2 = float(self.rc2)
         m.n_images = 1
         for k, v in self.consts.items():
             setattr(m, k, float(v))

@@ -201,6 +201,19 @@ __device__ __forceinline__ void walk_chain(const JrParams& P, Walker<G>& w, int 
       mwg_step<kExt>(P, w, s.step_key[t], s.step_move[t], emax, pressure, mu);
     w.g.sync();
   }
+  if constexpr (G::kFam == kFamSW) {
+    // the chain's pairs and triplets inside the cutoff, summed over threads
+    double a = w.tc[0], b = w.tc[1], c = w.tc[2], d = w.tc[3], z0 = 0.0, z1 = 0.0;
+    w.g.sum3(a, b, c, 1, w.par);
+    w.g.sum3(d, z0, z1, 1, w.par);
+    if (w.g.leader()) {
+      s.c_terms[0] += (long long)a;
+      s.c_terms[1] += (long long)b;
+      s.c_terms[2] += (long long)c;
+      s.c_terms[3] += (long long)d;
+    }
+    for (int q = 0; q < 4; ++q) w.tc[q] = 0;
+  }
 }
 
 // Copy the about-to-be-culled walker of replica p into info row `row`, cull
@@ -282,7 +295,8 @@ __device__ inline DynLayout dyn_layout(unsigned char* dyn, int K, int nmax, int 
 // (any NaN poisons it, culling walker 0), exact ties broken by the largest
 // uniform noise of that iteration's worst key, then the lowest index.
 __device__ inline void predict_fast(NsShared& ns, const double* E, int K, int Dr, Key key, Key key0,
-                             bool shared_mk) {
+                                    int mk_mode) {
+  const bool shared_mk = mk_mode != 0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (warp == 0) {
     Key kd = key;
@@ -308,7 +322,8 @@ __device__ inline void predict_fast(NsShared& ns, const double* E, int K, int Dr
     my_kw = split(kd, 1u);
     my_raw = randint(split(ka, 1u), 0, K - 1);
     ns.kmcmc[lane] = split(ka, 3u);
-    ns.kmove[lane] = shared_mk ? split(ns.k0chain[lane], 1u) : split(ka, 4u);
+    ns.kmove[lane] = mk_mode == 2 ? ns.k0chain[lane]
+                                  : (shared_mk ? split(ns.k0chain[lane], 1u) : split(ka, 4u));
   }
   const int nslot = (K + 31) >> 5;
   uint32_t taken = 0;
@@ -472,6 +487,13 @@ __device__ inline void select_culls_multi(NsShared& ns, const DynLayout& L, cons
   __syncthreads();
 }
 
+// The key of iteration d's move schedule: the run's own split(ka, 4)
+// (mode 0), fold_in(replica 0's key, 1) (mode 1, batched runs; k0d is replica
+// 0's key at iteration d), or the caller's explicit key (mode 2, k0d holds it).
+__device__ __forceinline__ Key move_schedule_key(int mode, Key k0d, Key kmoves) {
+  return mode == 2 ? k0d : (mode == 1 ? split(k0d, 1u) : kmoves);
+}
+
 template <class G>
 __device__ __forceinline__ G make_group(double (*red)[kMaxWarps][3]) {
   if constexpr (G::kIsWarp) {
@@ -545,7 +567,7 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
     __syncthreads();
     // ---- predictions for iterations d < Dr (every CTA, identically) ----
     const bool fast = ncull == 1 && nx == 0 && K <= 1024 && blockDim.x >= 64;
-    if (fast) predict_fast(ns, L.Epop, K, Dr, key, key0, D.shared_move_key != 0);
+    if (fast) predict_fast(ns, L.Epop, K, Dr, key, key0, D.shared_move_key);
     __syncthreads();
     Key kd = key, k0d = key0;
     for (int d = 0; d < (fast ? 0 : Dr); ++d) {
@@ -560,7 +582,7 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
           ns.clone[0] = ns.cc[0];
           ns.e[0] = ns.ce[ncull - 1];
           ns.kmcmc[0] = kmcmc;
-          ns.kmove[0] = D.shared_move_key ? split(k0d, 1u) : kmoves;
+          ns.kmove[0] = move_schedule_key(D.shared_move_key, k0d, kmoves);
         }
         __syncthreads();
         kd = split(ka, 0u);
@@ -588,7 +610,7 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
         ns.clone[d] = clone;
         ns.e[d] = emax;
         ns.kmcmc[d] = kmcmc;
-        ns.kmove[d] = D.shared_move_key ? split(k0d, 1u) : kmoves;
+        ns.kmove[d] = move_schedule_key(D.shared_move_key, k0d, kmoves);
         ns.wset[ns.n_wset++] = worst;
         for (int e = 0; e < nx; ++e) ns.wset[ns.n_wset++] = ns.extras[d * nx + e];
       }

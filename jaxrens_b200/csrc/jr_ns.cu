@@ -282,11 +282,20 @@ int jr_ns_iterate(const JrDims* dims, const JrParams* params, const JrStateBuffe
   }
   rc = check_config(c, dims, fam);
   if (rc) return rc;
+  if (dims->shared_move_key < 0 || dims->shared_move_key > 2)
+    return fail(JR_ERR_PARAM, "shared_move_key must be 0, 1 or 2");
+  if (dims->shared_move_key == 2 && (n_iter != 1 || !state->move_key))
+    return fail(JR_ERR_PARAM, "an explicit move key (shared_move_key = 2) needs "
+                              "state.move_key and n_iter = 1");
   JrInfoBuffers inf{};
   if (info) inf = *info;
   cudaStream_t s = (cudaStream_t)stream;
-  // snapshot of replica 0's key: the shared move schedule of every replica
-  cudaError_t e = cudaMemcpyAsync(workspace, state->rng_key, 2 * sizeof(uint32_t),
+  // the move-schedule key: a snapshot of replica 0's key (the shared move
+  // schedule of every replica, advanced per iteration in the kernel) or the
+  // caller's explicit key
+  const void* ksrc = dims->shared_move_key == 2 ? (const void*)state->move_key
+                                                : (const void*)state->rng_key;
+  cudaError_t e = cudaMemcpyAsync(workspace, ksrc, 2 * sizeof(uint32_t),
                                   cudaMemcpyDeviceToDevice, s);
   if (e != cudaSuccess) return cuda_fail(e, "key snapshot");
   if (fam == jr::kFamSW)
@@ -513,15 +522,19 @@ int restore_state(ScratchState& dst, const ScratchState& src, cudaStream_t st) {
 }  // namespace
 
 // Times every candidate launch shape on the same trajectory: a pristine copy
-// of the caller's state is taken once, and before each timed launch a working
+// of the caller's state is taken once, and before each timed sample a working
 // copy is restored from it, so every candidate walks the same iterations from
-// the same walkers (and meets the same speculation outcomes).  Each candidate
-// runs once untimed (compilation of its attributes, caches) and is then timed
-// kReps times; its score is the median.  The caller's state is not touched.
+// the same walkers (and meets the same speculation outcomes).  A sample is
+// kSegs consecutive launches of n_iter_probe iterations -- several segments of
+// the trajectory, since one launch's speculation outcome (one or two rounds)
+// varies from segment to segment.  Each candidate runs once untimed, then
+// kReps samples; its score is their median.  The caller's state is not
+// touched.
 extern "C" int jr_autotune(const JrDims* dims, const JrParams* params,
                            const JrStateBuffers* state, int32_t n_iter_probe,
                            JrLaunchConfig* best, void* stream) {
   constexpr int kReps = 3;
+  constexpr int kSegs = 4;
   int rc = check_params(dims, params);
   if (rc) return rc;
   if (!state || !best || n_iter_probe < 1) return fail(JR_ERR_PARAM, "autotune arguments");
@@ -564,10 +577,11 @@ extern "C" int jr_autotune(const JrDims* dims, const JrParams* params,
               cudaStreamSynchronize(st) == cudaSuccess;
     float ms[kReps];
     for (int r = 0; r < kReps && ok; ++r) {
-      ok = restore_state(work, pristine, st) == JR_OK && cudaEventRecord(e0, st) == cudaSuccess &&
-           jr_ns_iterate(dims, params, &work.b, nullptr, n_iter_probe, &c, ws, wsb, stream) ==
-               JR_OK &&
-           cudaEventRecord(e1, st) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+      ok = restore_state(work, pristine, st) == JR_OK && cudaEventRecord(e0, st) == cudaSuccess;
+      for (int g = 0; g < kSegs && ok; ++g)
+        ok = jr_ns_iterate(dims, params, &work.b, nullptr, n_iter_probe, &c, ws, wsb, stream) ==
+             JR_OK;
+      ok = ok && cudaEventRecord(e1, st) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
            cudaEventElapsedTime(&ms[r], e0, e1) == cudaSuccess;
     }
     if (!ok) {  // shape rejected or failed (e.g. too much shared memory): skip it

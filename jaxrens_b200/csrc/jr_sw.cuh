@@ -11,19 +11,20 @@
 // minimum image of the LJ path (dr - rint(dr . inv) . h).
 //
 // Evaluation, one walker, one thread group:
-//   1. pair pass over the n(n-1)/2 unordered pairs: minimum image, and for
-//      pairs inside r_c the per-pair record (dr, 1/r, g, u = g'/(g r), the
-//      two-body force coefficient c2 = phi2'/r) and the neighbour bits of
-//      both atoms; two-body energies summed;
-//   2. list pass (one warp): the neighbour pairs a < b in ascending (a, b)
-//      order, and the pair and triplet counts of the evaluation;
-//   3. triplet pass, one neighbour pair {a, b} per thread: V_ab = force on b
-//      from the triplets centred on a (other leg k ascending), V_ba likewise,
-//      and the triplet energies whose smaller leg is the pair's other atom
-//      (each triplet once); Q_ab = c2 dr_ab + V_ba - V_ab is the whole
+//   1. pair pass over the n(n-1)/2 unordered pairs: a cheap scan (minimum
+//      image, r^2 < rc2) sets the neighbour bits of both atoms and compacts
+//      the pairs inside the cutoff into per-warp segments, then every thread
+//      takes a share of those for the per-pair record (dr, 1/r, g,
+//      u = g'/(g r), the two-body force coefficient c2 = phi2'/r); two-body
+//      energies summed;
+//   2. triplet pass, the two centre sides of each neighbour pair {a, b} on
+//      two adjacent lanes: V_ab = force on b from the triplets centred on a
+//      (other leg k ascending) on one lane, V_ba likewise on the other, and
+//      the triplet energies whose smaller leg is the pair's other atom (each
+//      triplet once); Q_ab = c2 dr_ab + V_ba - V_ab is the whole
 //      antisymmetric pair share of the force, F_i = sum_j Q_ij;
-//   4. gather: F_i in the canonical order of the pair-matrix path (partners
-//      in blocks of 8, ascending, then the xor tree over the blocks).
+//   3. gather, one lane per atom: F_i = sum of +-Q_ij over the neighbours j
+//      of i in ascending order, sequentially in float32.
 // Every float32 operation is an explicit IEEE intrinsic; the CPU oracle's
 // DEV mode restates the same sequence, so forces match it bit for bit.  The
 // float64 energy sum of float32 terms is order-dependent here (terms near
@@ -77,14 +78,14 @@ __device__ __forceinline__ int sw_pidx(int lo, int hi, int n) {
   return lo * (2 * n - lo - 1) / 2 + (hi - lo - 1);
 }
 
-// Pair record of one pair inside the cutoff (float32, fixed op order):
-// r = sqrt(r2), 1/r, 1/(rc - r), the two exponentials, phi2, c2 = phi2'/r
-// and u = g'/(g r).  Returns false (nothing written) outside the cutoff.
-__device__ __forceinline__ bool sw_pair_terms(const SwConsts& c, float r2, float& inv_r, float& g,
+// Pair record of one pair inside the cutoff, r2 < rc2 (float32, fixed op
+// order): r = sqrt(r2), 1/r, 1/(rc - r), the two exponentials, phi2, c2 =
+// phi2'/r and u = g'/(g r).  The host sets rc2 to the largest float32 whose
+// correctly rounded square root lies below rc, so r < rc holds here.
+__device__ __forceinline__ void sw_pair_terms(const SwConsts& c, float r2, float& inv_r, float& g,
                                               float& u, float& c2, float& e2) {
-  if (!(r2 < c.rc2)) return false;
+  // r2 < rc2, and rc2 is chosen by the host so that then r < rc
   const float r = __fsqrt_rn(r2);
-  if (!(r < c.rc)) return false;
   inv_r = rcp_nr(r);
   const float md = __fsub_rn(c.rc, r);          // rc - r > 0
   const float inv_md = rcp_nr(md);
@@ -103,7 +104,6 @@ __device__ __forceinline__ bool sw_pair_terms(const SwConsts& c, float r2, float
   c2 = __fmul_rn(dphi, inv_r);
   // g'/g = -gamma sigma / (r - rc)^2
   u = __fmul_rn(-__fmul_rn(__fmul_rn(c.gsig, inv_md), inv_md), inv_r);
-  return true;
 }
 
 // One triplet seen from leg j of centre c (other leg k): the force on j
@@ -138,7 +138,7 @@ template <bool kForces>
 __device__ __forceinline__ void sw_side(const SwConsts& sc, const float4* r0, const float4* r1,
                                         uint64_t mask, int c, int j, int n, float jx, float jy,
                                         float jz, float ij, float gj, float uj, float& vx,
-                                        float& vy, float& vz, double& e3) {
+                                        float& vy, float& vz, double& e3, int& ntrip) {
   mask &= ~(1ull << j);
   while (mask) {
     const int k = __ffsll((long long)mask) - 1;
@@ -151,9 +151,37 @@ __device__ __forceinline__ void sw_side(const SwConsts& sc, const float4* r0, co
     if (kForces || k > j) {
       const float h = sw_triplet<kForces>(sc.leps, jx, jy, jz, ij, gj, uj, kx, ky, kz, a.w, b.x,
                                           vx, vy, vz);
-      if (k > j) e3 += (double)h;
+      if (k > j) {
+        e3 += (double)h;
+        ++ntrip;
+      }
     }
   }
+}
+
+// Neighbour bits of the pair (a, b) this lane scanned, if inside the cutoff
+// (native 32-bit shared atomics on the two halves of each 64-bit mask).
+__device__ __forceinline__ void sw_mask_bits(uint64_t* nbm, bool in, int a, int b) {
+  if (!in) return;
+  unsigned* m32 = reinterpret_cast<unsigned*>(nbm);
+  atomicOr(m32 + 2 * a + (b >> 5), 1u << (b & 31));
+  atomicOr(m32 + 2 * b + (a >> 5), 1u << (a & 31));
+}
+
+// Candidate q of the per-warp segments: `incl` is this lane's inclusive
+// prefix of the segment counts (lane l < nwarps holds warps 0..l), so the
+// segment of q is the number of lanes whose prefix is <= q.
+__device__ __forceinline__ int sw_cand_pair(const uint16_t* cand, int per_warp, int incl,
+                                            int nwarps, int q) {
+  int seg = 0, base = 0;
+  for (int l = 0; l < nwarps; ++l) {
+    const int il = __shfl_sync(0xffffffffu, incl, l);
+    if (q >= il) {
+      seg = l + 1;
+      base = il;
+    }
+  }
+  return cand[seg * per_warp + (q - base)];
 }
 
 // Energy (U) of the walker, forces into arr.F when kForces, and the sums
@@ -171,94 +199,116 @@ __device__ __forceinline__ void sw_eval(const JrParams& P, Walker<G>& w, const M
   uint64_t* nbm_next = arr.nbm + ((w.swpar + 1) & 1) * kSWMaxAtoms;
   w.swpar ^= 1;
   double ep = 0.0;
-  // ---- 1. pair pass ----
-  for (int p = tid; p < np; p += gs) {
+  const int lane = tid & 31, warp = tid >> 5, nwarps = gs >> 5;
+  const int per_warp = ((np + gs - 1) / gs) * 32;  // pairs one warp scans, at most
+  // ---- 1a. scan of every pair, two per trip with the loads of both issued
+  // first: minimum image and r^2.  The pairs inside the cutoff are appended
+  // to their warp's segment of the candidate list in scan order (so the list
+  // does not depend on timing), with (dr, r^2) in their record.
+  {
+    uint16_t* seg = arr.cand + warp * per_warp;
+    int cw = 0;
+    for (int p0 = warp * 32; p0 < np; p0 += 2 * gs) {
+      const int pa = p0 + lane, pb = p0 + gs + lane;
+      const bool va = pa < np, vb = pb < np;
+      const uint32_t aba = va ? arr.pij[pa] : 0u;
+      const uint32_t abb = vb ? arr.pij[pb] : 0u;
+      const float4 x0 = arr.xs[aba & 255], x1 = arr.xs[aba >> 8];
+      const float4 y0 = arr.xs[abb & 255], y1 = arr.xs[abb >> 8];
+      float ax = __fsub_rn(x1.x, x0.x), ay = __fsub_rn(x1.y, x0.y), az = __fsub_rn(x1.z, x0.z);
+      float bx = __fsub_rn(y1.x, y0.x), by = __fsub_rn(y1.y, y0.y), bz = __fsub_rn(y1.z, y0.z);
+      mic_r<kDiag>(cc, ax, ay, az);
+      mic_r<kDiag>(cc, bx, by, bz);
+      float ra2 = __fmul_rn(ax, ax);
+      ra2 = __fmaf_rn(ay, ay, ra2);
+      ra2 = __fmaf_rn(az, az, ra2);
+      float rb2 = __fmul_rn(bx, bx);
+      rb2 = __fmaf_rn(by, by, rb2);
+      rb2 = __fmaf_rn(bz, bz, rb2);
+      const bool ina = va && ra2 < sc.rc2, inb = vb && rb2 < sc.rc2;
+      const unsigned bala = __ballot_sync(0xffffffffu, ina);
+      const unsigned balb = __ballot_sync(0xffffffffu, inb);
+      const unsigned lt = (1u << lane) - 1u;
+      if (ina) {
+        seg[cw + __popc(bala & lt)] = (uint16_t)pa;
+        arr.swr0[pa] = make_float4(ax, ay, az, ra2);
+      }
+      cw += __popc(bala);
+      if (inb) {
+        seg[cw + __popc(balb & lt)] = (uint16_t)pb;
+        arr.swr0[pb] = make_float4(bx, by, bz, rb2);
+      }
+      cw += __popc(balb);
+      sw_mask_bits(nbm, ina, aba & 255, aba >> 8);
+      sw_mask_bits(nbm, inb, abb & 255, abb >> 8);
+    }
+    if (lane == 0) s.sw_cand[warp] = cw;
+  }
+  w.g.sync();
+  // prefix of the segment counts, in every warp (lane l: warps 0..l)
+  int incl = lane < nwarps ? s.sw_cand[lane] : 0;
+  for (int off = 1; off < 32; off <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += y;
+  }
+  const int M = __shfl_sync(0xffffffffu, incl, nwarps - 1);
+  // ---- 1b. pair records of the candidates, spread over every thread: r,
+  // 1/r, the exponentials, phi2, the force coefficients; neighbour bits.
+  uint16_t* dense = arr.cand + kSWCandDense;
+  for (int base = tid - lane; base < M; base += gs) {
+    const int q = base + lane;
+    const int p = sw_cand_pair(arr.cand, per_warp, incl, nwarps, q < M ? q : M - 1);
+    if (q < M) {
+      dense[q] = (uint16_t)p;
+      const float4 d = arr.swr0[p];
+      float inv_r, g, u, c2, e2;
+      sw_pair_terms(sc, d.w, inv_r, g, u, c2, e2);
+      arr.swr0[p] = make_float4(d.x, d.y, d.z, inv_r);
+      arr.swr1[p] = make_float4(g, u, c2, e2);
+      ep += (double)e2;
+      w.tc[kForces ? 0 : 2] += 1;
+    }
+  }
+  w.g.sync();
+  // ---- 2. triplet pass: the two centre sides of neighbour pair q on
+  // adjacent lanes (2q: centre a, 2q + 1: centre b), joined by one shuffle ----
+  for (int q = tid; q < n; q += gs) nbm_next[q] = 0ull;  // the next evaluation's masks
+  double e3 = 0.0;
+  int ntrip = 0;
+  for (int base = tid - lane; base < 2 * M; base += gs) {
+    const int u = base + lane;
+    const bool act = u < 2 * M;
+    const int side = u & 1;
+    const int p = act ? dense[u >> 1] : 0;
     const uint32_t ab = arr.pij[p];
     const int a = ab & 255, b = ab >> 8;
-    const float4 xa = arr.xs[a], xb = arr.xs[b];
-    float dx = __fsub_rn(xb.x, xa.x);
-    float dy = __fsub_rn(xb.y, xa.y);
-    float dz = __fsub_rn(xb.z, xa.z);
-    mic_r<kDiag>(cc, dx, dy, dz);
-    float r2 = __fmul_rn(dx, dx);
-    r2 = __fmaf_rn(dy, dy, r2);
-    r2 = __fmaf_rn(dz, dz, r2);
-    float inv_r, g, u, c2, e2;
-    if (sw_pair_terms(sc, r2, inv_r, g, u, c2, e2)) {
-      arr.swr0[p] = make_float4(dx, dy, dz, inv_r);
-      arr.swr1[p] = make_float4(g, u, c2, e2);
-      atomicOr(reinterpret_cast<unsigned long long*>(nbm + a), 1ull << b);
-      atomicOr(reinterpret_cast<unsigned long long*>(nbm + b), 1ull << a);
-      ep += (double)e2;
+    float vx = 0.0f, vy = 0.0f, vz = 0.0f;
+    float4 ra = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float c2 = 0.0f;
+    if (act) {
+      ra = arr.swr0[p];
+      const float4 rb = arr.swr1[p];
+      c2 = rb.z;
+      // side 0: V_ab, force on b from the triplets centred on a; side 1:
+      // V_ba, force on a from those centred on b (dr_ba = -dr_ab)
+      const float sg = side ? -1.0f : 1.0f;
+      sw_side<kForces>(sc, arr.swr0, arr.swr1, nbm[side ? b : a], side ? b : a, side ? a : b, n,
+                       sg * ra.x, sg * ra.y, sg * ra.z, ra.w, rb.x, rb.y, vx, vy, vz, e3, ntrip);
     }
-  }
-  w.g.sync();
-  // ---- 2. list pass: neighbour pairs in ascending (a, b) order (warp 0) ----
-  if (tid < 32) {
-    const int lane = tid;
-    const int a0 = lane, a1 = lane + 32;
-    const uint64_t m0 = a0 < n ? nbm[a0] : 0ull, m1 = a1 < n ? nbm[a1] : 0ull;
-    // partners above each atom
-    const uint64_t up0 = a0 >= 63 ? 0ull : (m0 >> (a0 + 1)) << (a0 + 1);
-    const uint64_t up1 = a1 >= 63 ? 0ull : (m1 >> (a1 + 1)) << (a1 + 1);
-    const int c0 = __popcll(up0), c1 = __popcll(up1);
-    // exclusive scan of c0 over lanes, then of c1 after all c0
-    int x0 = c0;
-    for (int off = 1; off < 32; off <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, x0, off);
-      if (lane >= off) x0 += y;
-    }
-    const int tot0 = __shfl_sync(0xffffffffu, x0, 31);
-    int x1 = c1;
-    for (int off = 1; off < 32; off <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, x1, off);
-      if (lane >= off) x1 += y;
-    }
-    const int tot1 = __shfl_sync(0xffffffffu, x1, 31);
-    int o0 = x0 - c0, o1 = tot0 + x1 - c1;
-    for (uint64_t m = up0; m; m &= m - 1)
-      arr.items[o0++] = (uint16_t)(a0 | ((__ffsll((long long)m) - 1) << 8));
-    for (uint64_t m = up1; m; m &= m - 1)
-      arr.items[o1++] = (uint16_t)(a1 | ((__ffsll((long long)m) - 1) << 8));
-    // pair and triplet counts of this evaluation
-    const int d0 = __popcll(m0), d1 = __popcll(m1);
-    int pairs = d0 + d1;
-    int trip = d0 * (d0 - 1) / 2 + d1 * (d1 - 1) / 2;
-    for (int off = 16; off > 0; off >>= 1) {
-      pairs += __shfl_xor_sync(0xffffffffu, pairs, off);
-      trip += __shfl_xor_sync(0xffffffffu, trip, off);
-    }
-    if (lane == 0) {
-      s.sw_nitems = tot0 + tot1;
-      s.c_terms[kForces ? 0 : 2] += pairs / 2;
-      s.c_terms[kForces ? 1 : 3] += trip;
-    }
-  }
-  w.g.sync();
-  // ---- 3. triplet pass ----
-  const int nitems = s.sw_nitems;
-  double e3 = 0.0;
-  for (int q = tid; q < n; q += gs) nbm_next[q] = 0ull;  // the next evaluation's masks
-  for (int q = tid; q < nitems; q += gs) {
-    const uint32_t it = arr.items[q];
-    const int a = it & 255, b = it >> 8;
-    const int p = sw_pidx(a, b, n);
-    const float4 ra = arr.swr0[p];
-    const float4 rb = arr.swr1[p];
-    float vabx = 0.0f, vaby = 0.0f, vabz = 0.0f;  // force on b, centre a
-    float vbax = 0.0f, vbay = 0.0f, vbaz = 0.0f;  // force on a, centre b
-    sw_side<kForces>(sc, arr.swr0, arr.swr1, nbm[a], a, b, n, ra.x, ra.y, ra.z, ra.w, rb.x, rb.y,
-                     vabx, vaby, vabz, e3);
-    sw_side<kForces>(sc, arr.swr0, arr.swr1, nbm[b], b, a, n, -ra.x, -ra.y, -ra.z, ra.w, rb.x,
-                     rb.y, vbax, vbay, vbaz, e3);
     if (kForces) {
-      // Q_ab = c2 dr_ab + V_ba - V_ab
-      const float qx = __fsub_rn(__fmaf_rn(rb.z, ra.x, vbax), vabx);
-      const float qy = __fsub_rn(__fmaf_rn(rb.z, ra.y, vbay), vaby);
-      const float qz = __fsub_rn(__fmaf_rn(rb.z, ra.z, vbaz), vabz);
-      arr.swq[p] = make_float4(qx, qy, qz, 0.0f);
+      const float ox = __shfl_xor_sync(0xffffffffu, vx, 1);
+      const float oy = __shfl_xor_sync(0xffffffffu, vy, 1);
+      const float oz = __shfl_xor_sync(0xffffffffu, vz, 1);
+      if (act && side == 0) {
+        // Q_ab = c2 dr_ab + V_ba - V_ab
+        const float qx = __fsub_rn(__fmaf_rn(c2, ra.x, ox), vx);
+        const float qy = __fsub_rn(__fmaf_rn(c2, ra.y, oy), vy);
+        const float qz = __fsub_rn(__fmaf_rn(c2, ra.z, oz), vz);
+        arr.swq[p] = make_float4(qx, qy, qz, 0.0f);
+      }
     }
   }
+  w.tc[kForces ? 1 : 3] += ntrip;
   ep += e3;
   if (!kForces) {
     double z0 = 0.0, z1 = 0.0;
@@ -269,42 +319,29 @@ __device__ __forceinline__ void sw_eval(const JrParams& P, Walker<G>& w, const M
     return;
   }
   w.g.sync();
-  // ---- 4. gather: F_i = sum_j Q_ij, partners in blocks of 8 ascending ----
-  const int L = gather_lanes(n);
-  const int apb = gs / L;
-  const int blk = tid & (L - 1);
-  for (int off = 1; off < L; off <<= 1) ep += __shfl_xor_sync(0xffffffffu, ep, off);
+  // ---- 3. gather, one lane per atom: F_i = sum over the neighbours j of i
+  // in ascending order of +-Q, a sequential float32 sum from +0 ----
   double ff_part = 0.0, fd_part = 0.0;
-  for (int base = 0; base < n; base += apb) {
-    const int i = base + tid / L;
-    if (!__any_sync(0xffffffffu, i < n)) continue;
+  for (int i = tid; i < n; i += gs) {
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-    const int j0 = blk * 8;
-    if (i < n && j0 < n) {
-      uint64_t m = (nbm[i] >> j0) & 0xffull;
-      while (m) {
-        const int j = j0 + __ffsll((long long)m) - 1;
-        m &= m - 1;
-        const bool fwd = i < j;
-        const float4 q = arr.swq[fwd ? sw_pidx(i, j, n) : sw_pidx(j, i, n)];
-        fx = __fadd_rn(fx, fwd ? q.x : -q.x);
-        fy = __fadd_rn(fy, fwd ? q.y : -q.y);
-        fz = __fadd_rn(fz, fwd ? q.z : -q.z);
-      }
+    for (uint64_t m = nbm[i]; m; m &= m - 1) {
+      const int j = __ffsll((long long)m) - 1;
+      const bool fwd = i < j;
+      const float4 q = arr.swq[fwd ? sw_pidx(i, j, n) : sw_pidx(j, i, n)];
+      fx = __fadd_rn(fx, fwd ? q.x : -q.x);
+      fy = __fadd_rn(fy, fwd ? q.y : -q.y);
+      fz = __fadd_rn(fz, fwd ? q.z : -q.z);
     }
-    gather_tree(fx, fy, fz, L);
-    if (blk == 0 && i < n) {
-      arr.F[3 * i] = fx;
-      arr.F[3 * i + 1] = fy;
-      arr.F[3 * i + 2] = fz;
-      const double dx = fx, dy = fy, dz = fz;
-      ff_part = __fma_rn(dx, dx, __fma_rn(dy, dy, __fma_rn(dz, dz, ff_part)));
-      fd_part = __fma_rn(dx, (double)arr.dir[3 * i],
-                         __fma_rn(dy, (double)arr.dir[3 * i + 1],
-                                  __fma_rn(dz, (double)arr.dir[3 * i + 2], fd_part)));
-    }
+    arr.F[3 * i] = fx;
+    arr.F[3 * i + 1] = fy;
+    arr.F[3 * i + 2] = fz;
+    const double dx = fx, dy = fy, dz = fz;
+    ff_part = __fma_rn(dx, dx, __fma_rn(dy, dy, __fma_rn(dz, dz, ff_part)));
+    fd_part = __fma_rn(dx, (double)arr.dir[3 * i],
+                       __fma_rn(dy, (double)arr.dir[3 * i + 1],
+                                __fma_rn(dz, (double)arr.dir[3 * i + 2], fd_part)));
   }
-  w.g.sum3(ep, ff_part, fd_part, L, w.par);
+  w.g.sum3(ep, ff_part, fd_part, 1, w.par);
   U = ep;
   sff = ff_part;
   sfd = fd_part;

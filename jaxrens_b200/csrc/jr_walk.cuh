@@ -53,6 +53,9 @@ __device__ __forceinline__ StepKey make_step_key(Key k) {
 // normals of a chunk of steps (kStepChunk x 3 n floats).
 constexpr int kNormalAtomsMax = 32;
 constexpr int kSWMaxAtoms = 64;  // Stillinger-Weber walkers: one 64-bit neighbour mask per atom
+constexpr int kSWCandSlack = 16 * 32;  // per-warp segment rounding of the SW candidate list
+// offset of the dense candidate list after the per-warp segments
+constexpr int kSWCandDense = kSWMaxAtoms * (kSWMaxAtoms - 1) / 2 + kSWCandSlack;
 constexpr int kPairMatMax = 96;  // walkers up to this size use the pair matrix
                                  // (12 n pm_stride(n) bytes: 112 KB at 96; measured faster than
                                  // the ordered pairs from 32 to 96 atoms)
@@ -163,7 +166,7 @@ struct WalkShared {
   StepKey step_key[kStepChunk];
   int step_move[kStepChunk];
   int cell_ok;  // cell-geometry verdict of the pending cell move
-  int sw_nitems;  // Stillinger-Weber: neighbour pairs of the current evaluation
+  int sw_cand[kMaxWarps];  // Stillinger-Weber: pairs inside the cutoff found by each warp
   // Stillinger-Weber: pairs and triplets inside the cutoff summed over the
   // chain's evaluations, [energy+forces pairs, triplets, energy-only pairs,
   // triplets] (the algorithmic work of the chain)
@@ -203,7 +206,8 @@ struct WalkArrays {
   float4* swr1;         // [n(n-1)/2] (g, g'/(g r), phi2'/r, phi2)
   float4* swq;          // [n(n-1)/2] pair force share Q_ab
   uint64_t* nbm;        // [2][kSWMaxAtoms] neighbour masks (alternating evaluations)
-  uint16_t* items;      // [n(n-1)/2] neighbour pairs a | b << 8
+  uint16_t* cand;       // [kSWCandDense + n(n-1)/2] pairs inside the cutoff: per-warp
+                        // segments, then (from kSWCandDense) the dense list
 };
 
 __host__ __device__ inline bool use_pair_matrix(int nmax, int nimg, int fam = kFamPair) {
@@ -233,7 +237,8 @@ __host__ __device__ inline bool use_normal_buffer(int nmax, bool normals) {
 // Bytes of the Stillinger-Weber tables of one walker.
 __host__ __device__ inline size_t sw_table_bytes(int nmax) {
   const size_t np = pair_count(nmax);
-  return 3u * 16u * np + 2u * 8u * (size_t)kSWMaxAtoms + align16(2u * np);
+  return 3u * 16u * np + 2u * 8u * (size_t)kSWMaxAtoms +
+         align16(2u * ((size_t)kSWCandDense + np));
 }
 
 __host__ __device__ inline size_t walker_smem_bytes(int nmax, int nimg, bool normals = false,
@@ -269,7 +274,7 @@ __device__ inline WalkShared* carve_walker(char* p, int nmax, int nimg, const ui
   a.pij = nullptr;
   a.swr0 = a.swr1 = a.swq = nullptr;
   a.nbm = nullptr;
-  a.items = nullptr;
+  a.cand = nullptr;
   if (use_pair_matrix(nmax, nimg, fam)) {
     a.pm = (float*)p;
     a.pij = pij;
@@ -282,7 +287,7 @@ __device__ inline WalkShared* carve_walker(char* p, int nmax, int nimg, const ui
     a.swr1 = (float4*)p; p += 16u * np;
     a.swq = (float4*)p; p += 16u * np;
     a.nbm = (uint64_t*)p; p += 2u * 8u * kSWMaxAtoms;
-    a.items = (uint16_t*)p; p += align16(2u * np);
+    a.cand = (uint16_t*)p; p += align16(2u * ((size_t)kSWCandDense + np));
   }
   a.nz = use_normal_buffer(nmax, normals) ? (float*)p : nullptr;
   return s;
@@ -326,6 +331,9 @@ struct Walker {
   G g;
   int par;
   int swpar = 0;  // Stillinger-Weber: which neighbour-mask buffer the next evaluation uses
+  // Stillinger-Weber: this thread's share of the pairs and triplets inside
+  // the cutoff since the chain began (energy+forces, then energy-only)
+  int tc[4] = {0, 0, 0, 0};
 };
 
 __device__ __forceinline__ float& pos_at(float4* xs, int idx) {

@@ -299,8 +299,11 @@ class InfoBuffers:
 
 def ns_iterate(ns_state: NSState, step_fn: MWGStep, n_iter: int, n_mcmc_steps: int = 20,
                n_extra: int = 0, n_cull: int = 1, info: InfoBuffers | None = None,
-               cfg: _lib.JrLaunchConfig | None = None) -> InfoBuffers:
-    """Run ``n_iter`` NS iterations on every run in one launch."""
+               cfg: _lib.JrLaunchConfig | None = None, move_key=None) -> InfoBuffers:
+    """Run ``n_iter`` NS iterations on every run in one launch.  ``move_key``
+    (one iteration only): the key of the move schedule, ``split(move_key,
+    n_mcmc_steps)``, shared by every run, as the reference's ``ns_step``
+    takes it; by default the schedule comes from the run keys."""
     K = ns_state.n_walkers
     la = prior_mass.log_alpha(K, n_cull)
     _, w_off = prior_mass.iteration_offsets(K, n_cull)
@@ -311,6 +314,16 @@ def ns_iterate(ns_state: NSState, step_fn: MWGStep, n_iter: int, n_mcmc_steps: i
     if info.n_cull != n_cull:
         raise ValueError("info buffers were sized for a different n_cull")
     sb = state_buffers(ns_state)
+    mk_dev = None
+    if move_key is not None:
+        import torch
+
+        if n_iter != 1:
+            raise ValueError("an explicit move_key drives exactly one iteration")
+        words = np.asarray(move_key, np.uint32).reshape(2)
+        mk_dev = torch.as_tensor(words.view(np.int32).copy(), device=ns_state.rng_key.device)
+        dims.shared_move_key = 2
+        sb.move_key = mk_dev.data_ptr()
     ib = info.cstruct()
     rc = _lib.load().jr_ns_iterate(
         C.byref(dims), C.byref(params), C.byref(sb), C.byref(ib), int(n_iter),
@@ -370,10 +383,10 @@ def ns_step(ns_state: NSState, step_fn: MWGStep, n_mcmc_steps: int = 20, n_extra
             n_cull: int = 1, move_key=None):
     """One NS iteration (``nested_sampling.py:391-686``); returns
     ``(ns_state, info)``.  The run key and (for batched runs) the shared move
-    schedule are derived on the device exactly as the reference does."""
-    if move_key is not None:
-        raise NotImplementedError("the move schedule key is derived from the run keys")
-    info = ns_iterate(ns_state, step_fn, 1, n_mcmc_steps, n_extra, n_cull)
+    schedule are derived on the device exactly as the reference does; a
+    caller's ``move_key`` (the reference batcher's ``_shared_move_key``,
+    ``batch_descriptor.py:177-195``) replaces the schedule key for every run."""
+    info = ns_iterate(ns_state, step_fn, 1, n_mcmc_steps, n_extra, n_cull, move_key=move_key)
     return ns_state, info_dict(info, ns_state, n_mcmc_steps, n_extra, 0)
 
 

@@ -74,6 +74,11 @@ def uniform(k, n: int) -> np.ndarray:
     return (f - np.float32(1.0)).astype(np.float32)
 
 
+def bernoulli(k, n: int, p: float = 0.5) -> np.ndarray:
+    """``jax.random.bernoulli(k, p, (n,))``: ``uniform(k, (n,)) < p``."""
+    return uniform(k, n) < np.float32(p)
+
+
 def advance_iteration(k) -> np.ndarray:
     """The run key after one ns_step iteration (nested_sampling.py:465-466)."""
     return split(split(k, 2)[0], 5)[0]

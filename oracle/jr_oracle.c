@@ -548,9 +548,10 @@ static inline int sw_pidx(int lo, int hi, int n) { return lo * (2 * n - lo - 1) 
 
 /* The kernel's pair record (float32, the kernel's op order). */
 static int sw_pair_dev(const JroModel* m, float r2, SwPair* q) {
+  /* rc2 is the smallest float32 whose square root reaches rc, so r2 < rc2
+   * is exactly sqrt(r2) < rc */
   if (!(r2 < m->rc2)) return 0;
   const float r = sqrtf(r2);
-  if (!(r < m->sw_rc)) return 0;
   q->inv_r = rcp_nr(r);
   const float md = m->sw_rc - r;
   const float inv_md = rcp_nr(md);
@@ -591,7 +592,7 @@ static float sw_triplet_dev(float leps, const float* jv, float ij, float gj, flo
 
 /* The kernel contract (DEV): pair records, per neighbour pair {a<b} the two
  * centre sides with the other leg ascending, Q_ab = c2 dr_ab + V_ba - V_ab,
- * F_i gathered over neighbours in blocks of 8 then the pairwise tree.  Also
+ * F_i the sequential float32 sum of +-Q_ij over the neighbours j ascending.  Also
  * used for REF32: the reference has no Stillinger-Weber to take an op order
  * from.  *n_pairs / *n_trip receive the evaluation's counts (may be NULL). */
 static double sw_dev(const JroModel* m, int n, const float* x, const float* cell_in, double* F,
@@ -678,27 +679,15 @@ static double sw_dev(const JroModel* m, int n, const float* x, const float* cell
       }
     }
   if (F) {
-    int nb = (n + 7) / 8, L = 1;
-    while (L < nb) L <<= 1;
     for (int i = 0; i < n; ++i) {
-      float Pb[32][3];
-      memset(Pb, 0, sizeof(Pb));
-      for (int bk = 0; bk < L; ++bk) {
-        const int j0 = 8 * bk, j1 = j0 + 8 < n ? j0 + 8 : n;
-        for (int j = j0; j < j1; ++j) {
-          if (!((nbm[i] >> j) & 1ull)) continue;
-          const int fwd = i < j;
-          const float* qv = Q + 3 * (fwd ? sw_pidx(i, j, n) : sw_pidx(j, i, n));
-          for (int q = 0; q < 3; ++q) Pb[bk][q] = Pb[bk][q] + (fwd ? qv[q] : -qv[q]);
-        }
+      float f[3] = {0.0f, 0.0f, 0.0f};
+      for (int j = 0; j < n; ++j) {
+        if (!((nbm[i] >> j) & 1ull)) continue;
+        const int fwd = i < j;
+        const float* qv = Q + 3 * (fwd ? sw_pidx(i, j, n) : sw_pidx(j, i, n));
+        for (int q = 0; q < 3; ++q) f[q] = f[q] + (fwd ? qv[q] : -qv[q]);
       }
-      for (int st = 1; st < L; st <<= 1) {
-        float T2[32][3];
-        for (int bk = 0; bk < L; ++bk)
-          for (int q = 0; q < 3; ++q) T2[bk][q] = Pb[bk][q] + Pb[bk ^ st][q];
-        memcpy(Pb, T2, sizeof(float) * 3 * L);
-      }
-      for (int q = 0; q < 3; ++q) F[3 * i + q] = (double)Pb[0][q];
+      for (int q = 0; q < 3; ++q) F[3 * i + q] = (double)f[q];
     }
   }
   free(pr);

@@ -281,9 +281,21 @@ def make_sw_model(sw_sigma, sw_rc, sw_gsig, sw_Aeps, sw_B, sw_leps) -> JroModel:
     m.has_cutoff = 1
     m.sw_sigma, m.sw_rc, m.sw_gsig = (float(np.float32(v)) for v in (sw_sigma, sw_rc, sw_gsig))
     m.sw_Aeps, m.sw_B, m.sw_leps = (float(np.float32(v)) for v in (sw_Aeps, sw_B, sw_leps))
-    m.rc2 = np.float32(np.float32(sw_rc) * np.float32(sw_rc))
+    m.rc2 = sw_cutoff_sq(sw_rc)
     m.n_images = 1
     return m
+
+
+def sw_cutoff_sq(rc) -> np.float32:
+    """The smallest float32 x whose float32 square root reaches rc: then
+    r2 < x is exactly sqrt(r2) < rc."""
+    rc = np.float32(rc)
+    x = np.float32(rc * rc)
+    while np.sqrt(x) >= rc:
+        x = np.nextafter(x, np.float32(0))
+    while np.sqrt(x) < rc:
+        x = np.nextafter(x, np.float32(np.inf))
+    return x
 
 
 def sw_exp(x: float) -> float:

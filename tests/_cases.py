@@ -69,13 +69,14 @@ def lj_case(P=1, K=32, N=8, seed=0, n_reflect=4, T=5, pressure=0.1, epsilon=1.0,
     root = prng.key(seed)
     keys = prng.split(root, P + 1)
     pos, cells, types = [], [], []
-    rng = np.random.default_rng(seed)
     for r in range(P):
         p_, c_ = jinit.uniform_gas(keys[r], K, Ns[r], v_hi_per_atom * Ns[r])
         pos.append(p_)
         cells.append(c_)
         if S > 1:
-            types.append(rng.integers(0, S, size=(K, Ns[r])).astype(np.int32))
+            # species uniform over S from threefry bits of a per-run key
+            u = prng.uniform(prng.fold_in(keys[r], 7), K * Ns[r])
+            types.append(np.minimum((u * S).astype(np.int32), S - 1).reshape(K, Ns[r]))
         else:
             types.append(np.zeros((K, Ns[r]), np.int32))
     run_keys = prng.split(keys[P], P)

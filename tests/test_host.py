@@ -306,3 +306,32 @@ def test_oracle_shear_and_stretch_preserve_volume_and_fractions():
     with pytest.raises(NotImplementedError):
         build_mwg(create_lj(), [mv_.volume_move(4, min_aspect_ratio=0.8),
                                 mv_.shear_move(4, min_aspect_ratio=0.5)])
+
+
+def test_uniform_gas_matches_the_oracle_bit_for_bit():
+    """The host's synthetic initial walkers (init.uniform_gas) against the
+    oracle's restatement (jro_init_walkers): cubic cell of volume
+    v_hi * (1 - u), fractional coordinates uniform, walker k from
+    split(key, K)[k] -- the same float32 values."""
+    from jaxrens_b200 import init as jinit
+    from jaxrens_b200 import prng
+    from oracle import oracle as O
+
+    for seed, K, N, v in ((0, 17, 8, 64.0), (5, 9, 32, 256.0), (11, 4, 64, 64 * 160.0)):
+        key = prng.key(seed)
+        p_host, c_host = jinit.uniform_gas(key, K, N, v)
+        p_or, c_or = O.init_walkers(key, K, N, v)
+        np.testing.assert_array_equal(p_host, p_or)
+        np.testing.assert_array_equal(c_host, c_or)
+
+
+def test_bernoulli_species_draws():
+    """Species Bernoulli(0.5) from a threefry key: uniform(key, n) < 0.5,
+    the same bits as the oracle's uniform stream."""
+    from jaxrens_b200 import prng
+    from oracle import oracle as O
+
+    k = prng.key(3)
+    b = prng.bernoulli(k, 4096, 0.5)
+    np.testing.assert_array_equal(b, O.uniform(k, 4096) < np.float32(0.5))
+    assert abs(b.mean() - 0.5) < 0.03
