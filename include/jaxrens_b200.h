@@ -175,9 +175,12 @@ typedef struct JrInfoBuffers {
   int32_t* n_grad_evaluations;     /* [n_iter][P][M] */
   int32_t* rounds;                 /* [P] speculation rounds used (diagnostic) */
   double* dead_energy;             /* [n_iter][P][n_cull] energies of the culled walkers */
-  /* [n_iter][P][4] Stillinger-Weber work of the iteration's chains: pairs and
-   * triplets inside the cutoff summed over the energy+force evaluations, then
-   * over the energy-only ones (zero for the other models) */
+  /* [n_iter][P][4] work the iteration's chains evaluated: pairs and
+   * triplets of the evaluations with forces, then of the energy-only ones.
+   * Pairs are LJ's unique interactions (every image) or Stillinger-Weber's
+   * pairs inside the cutoff; triplets are Stillinger-Weber's (zero for LJ).
+   * A galilean step evaluates the energy and, only when it reflects off the
+   * contour, the forces. */
   int64_t* term_counts;
 } JrInfoBuffers;
 

@@ -201,8 +201,8 @@ __device__ __forceinline__ void walk_chain(const JrParams& P, Walker<G>& w, int 
       mwg_step<kExt>(P, w, s.step_key[t], s.step_move[t], emax, pressure, mu);
     w.g.sync();
   }
-  if constexpr (G::kFam == kFamSW) {
-    // the chain's pairs and triplets inside the cutoff, summed over threads
+  {
+    // the chain's evaluated pairs and triplets, summed over threads
     double a = w.tc[0], b = w.tc[1], c = w.tc[2], d = w.tc[3], z0 = 0.0, z1 = 0.0;
     w.g.sum3(a, b, c, 1, w.par);
     w.g.sum3(d, z0, z1, 1, w.par);

@@ -167,9 +167,9 @@ struct WalkShared {
   int step_move[kStepChunk];
   int cell_ok;  // cell-geometry verdict of the pending cell move
   int sw_cand[kMaxWarps];  // Stillinger-Weber: pairs inside the cutoff found by each warp
-  // Stillinger-Weber: pairs and triplets inside the cutoff summed over the
-  // chain's evaluations, [energy+forces pairs, triplets, energy-only pairs,
-  // triplets] (the algorithmic work of the chain)
+  // work of the chain's evaluations: [pairs with forces, triplets with
+  // forces, energy-only pairs, energy-only triplets]; pairs are LJ's unique
+  // interactions or Stillinger-Weber's pairs inside the cutoff
   long long c_terms[4];
   // pre-move copy for the constraint gate
   double E_save;
@@ -331,8 +331,9 @@ struct Walker {
   G g;
   int par;
   int swpar = 0;  // Stillinger-Weber: which neighbour-mask buffer the next evaluation uses
-  // Stillinger-Weber: this thread's share of the pairs and triplets inside
-  // the cutoff since the chain began (energy+forces, then energy-only)
+  // this thread's share of the chain's evaluated work since the chain began:
+  // pairs (LJ: unique interactions; Stillinger-Weber: pairs inside the
+  // cutoff) and triplets, with forces, then energy-only
   int tc[4] = {0, 0, 0, 0};
 };
 
@@ -680,6 +681,7 @@ __device__ __forceinline__ void pairs_matrix(const JrParams& P, Walker<G>& w, co
       if (two) put(a1, b1, vx1, vy1, vz1);
     }
   }
+  if (tid == 0) w.tc[kForces ? 0 : 2] += np;
   if (!kForces) {
     double z0 = 0.0, z1 = 0.0;
     w.g.sum3(ep, z0, z1, 1, w.par);
@@ -772,6 +774,9 @@ __device__ __forceinline__ void pairs_ordered(const JrParams& P, Walker<G>& w, c
   const int apb = w.g.size() / L;
   const int blk = tid & (L - 1);
   const int center = center_image(mp);
+  // unique interactions: every image of every pair once, no self term in
+  // the centre image
+  if (tid == 0) w.tc[kForces ? 0 : 2] += (nimg * n * n - n) / 2;
   double e_part = 0.0, ff_part = 0.0, fd_part = 0.0;
   for (int base = 0; base < n; base += apb) {
     const int i = base + tid / L;
@@ -966,15 +971,20 @@ __device__ __forceinline__ double galilean_trajectory(const JrParams& P, Walker<
       x = __fmaf_rn(step, d, x);
     }
     w.g.sync();
-    double U, sff, sfd;
+    // Forces only steer a reflection, so each step first evaluates the
+    // energy alone and evaluates the forces (at the same positions) only when
+    // the step lands on or above the contour -- a few percent of the steps
+    // on the benchmark workloads.  The walk is the same as evaluating both
+    // every step: the decision reads the energy, the reflection the forces.
+    double U, sff = 0.0, sfd = 0.0;
     if constexpr (kPath == kTrajSW) {
-      sw_eval<true, kDiag>(P, w, cc, U, sff, sfd);
+      sw_eval<false, kDiag>(P, w, cc, U, sff, sfd);
       E = U + ens;
     } else if (kPath == kTrajMatrix) {
-      pairs_matrix<true, kS1, kDiag>(P, w, cc, U, sff, sfd);
+      pairs_matrix<false, kS1, kDiag>(P, w, cc, U, sff, sfd);
       E = U + ens;
     } else if (kPath == kTrajOrdered) {
-      pairs_ordered<true, kS1, kDiag>(P, w, cc, T, U, sff, sfd);
+      pairs_ordered<false, kS1, kDiag>(P, w, cc, T, U, sff, sfd);
       E = U + ens;
     } else {
       model_eval<true>(P, w, cidx, U, sff, sfd);
@@ -983,6 +993,10 @@ __device__ __forceinline__ double galilean_trajectory(const JrParams& P, Walker<
     if (isnan(E)) E = INFINITY;
     refl = E >= emax;
     if (refl) {
+      if constexpr (kPath == kTrajSW) sw_eval<true, kDiag>(P, w, cc, U, sff, sfd);
+      else if constexpr (kPath == kTrajMatrix) pairs_matrix<true, kS1, kDiag>(P, w, cc, U, sff, sfd);
+      else if constexpr (kPath == kTrajOrdered)
+        pairs_ordered<true, kS1, kDiag>(P, w, cc, T, U, sff, sfd);
       // d <- d - [2 (F.d) / max(|F|^2, 1e-20)] F, the scalar in float32
       const float ffs = __double2float_rn(sff);
       coef = __fmul_rn(2.0f * __double2float_rn(sfd), rcp_nr(ffs > 1e-20f ? ffs : 1e-20f));

@@ -402,3 +402,21 @@ def test_move_trials_match_oracle():
                                          rep.positions[k], rep.direction[k], rep.types[k],
                                          rep.cell[k], rep.energy[k], pressure=rep.pressure)
                 assert bool(acc[r, t]) == a
+
+
+def test_lazy_forces_work_counters():
+    """A galilean step evaluates the energy and, only when it reflects off the
+    contour, the forces: per iteration the energy-only pair count is exactly
+    every counted evaluation's n(n-1)/2 unique pairs, and the pairs with
+    forces are n(n-1)/2 per reflection, at most one per counted gradient
+    evaluation.  The walk itself is pinned to the oracle by the other tests."""
+    case = lj_case(P=2, K=24, N=12, seed=77, n_reflect=5, T=6)
+    ns, infos = _run_gpu(case, 8, 6)
+    np_ = 12 * 11 // 2
+    for info in infos:
+        tc = _np(info.term_counts)
+        ne = _np(info.n_evaluations).sum(-1)
+        ng = _np(info.n_grad_evaluations).sum(-1)
+        np.testing.assert_array_equal(tc[..., 2], ne * np_)
+        assert (tc[..., 0] % np_ == 0).all() and (tc[..., 0] <= ng * np_).all()
+        assert (tc[..., 1] == 0).all() and (tc[..., 3] == 0).all()

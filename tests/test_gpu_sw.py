@@ -78,11 +78,15 @@ def test_sw_batched_64_atoms_matches_oracle():
     ns, infos = _run_gpu(case, 6, 3)
     reps, hist = _run_oracle(case, 6, 3)
     _compare(case, ns, infos, reps, hist)
-    # the evaluation counters of the iterations: every energy+force evaluation
-    # sees at most n(n-1)/2 pairs and at least one
+    # the work counters of the iterations: every step evaluates the energy
+    # (at most n(n-1)/2 pairs each); forces are evaluated only on the
+    # galilean steps that reflect, at most once per counted evaluation
     tc = np.concatenate([_np(i.term_counts) for i in infos])
+    ne = np.concatenate([_np(i.n_evaluations).sum(-1) for i in infos])
     ng = np.concatenate([_np(i.n_grad_evaluations).sum(-1) for i in infos])
-    assert (tc[..., 0] > 0).all() and (tc[..., 0] <= ng * 64 * 63 // 2).all()
+    assert (tc[..., 2] > 0).all() and (tc[..., 2] <= ne * 64 * 63 // 2).all()
+    assert (tc[..., 0] <= ng * 64 * 63 // 2).all()
+    assert (tc[..., 1] <= ng * 64 * 63 * 62).all() and (tc[..., 3] >= 0).all()
 
 
 def test_sw_launch_shapes_agree():
