@@ -281,6 +281,53 @@ int jr_autotune(const JrDims* dims, const JrParams* params,
                 const JrStateBuffers* state, int32_t n_iter_probe,
                 JrLaunchConfig* best, void* stream);
 
+/* ---- learned surrogate and the delayed-acceptance walk ----
+ * None of these has a counterpart in the reference: the surrogate is a
+ * learned energy the walk trains on configurations it evaluated exactly, and
+ * uses to screen galilean and volume proposals (two-stage delayed
+ * acceptance: the smoothed surrogate constraint first, the exact potential
+ * deciding every step).  Descriptors: 16 Gaussian radial functions per atom
+ * (centres 1.5..3.8 A, cosine cutoff 3.8 A); network 16-64-64-1 with SiLU,
+ * bfloat16 weights and activations in the products, float32 accumulation. */
+#define JR_SUR_BASIS 16
+#define JR_SUR_HIDDEN 64
+/* float32 parameters, flat: W1[16][64] b1[64] W2[64][64] b2[64] w3[64] b3 */
+#define JR_SUR_PARAMS 5313
+
+typedef struct JrSurrogate {
+  const float* params;       /* device, [JR_SUR_PARAMS] */
+  float in_scale[JR_SUR_BASIS], in_shift[JR_SUR_BASIS]; /* x = D in_scale + in_shift */
+  float out_scale, out_shift; /* U = sum_i (e_i out_scale + out_shift) */
+  float contour_shift;       /* surrogate contour: emax + contour_shift */
+  float tau;                 /* width of the smoothed surrogate constraint */
+} JrSurrogate;
+
+/* Descriptors D [n_configs][n_atoms][16] (float32) of configurations
+ * positions [n_configs][n_atoms][3], cell [n_configs][9] (device),
+ * n_atoms <= 128. */
+int jr_sur_descriptors(int32_t n_configs, int32_t n_atoms, const float* positions,
+                       const float* cell, float* descriptors, void* stream);
+
+/* Device workspace bytes of jr_sur_train_step for a batch of n_batch
+ * configurations. */
+size_t jr_sur_train_workspace_size(int32_t n_batch, int32_t n_atoms);
+
+/* One Adam step of the surrogate on n_batch configurations: batch_idx
+ * [n_batch] picks rows of descriptors [*][n_atoms][16] and targets
+ * energy_u [*] (the model energy U).  Loss: mean over the batch of
+ * ((sum_i e_i out_scale + n out_shift - U) / n)^2.  params, adam_m, adam_v
+ * [JR_SUR_PARAMS] are updated in place (step counts from 1); *loss (device)
+ * receives the batch loss before the update.  Forward and backward run on
+ * the tensor cores (tcgen05, accumulators in tensor memory).  n_atoms must
+ * be 64 (two configurations per 128-row tile).  Workspace layout: an int32
+ * error flag (set to 1 if a bounded tensor-core wait gave up; the step's
+ * update is then not valid), padded to 256 bytes, then the per-CTA gradient
+ * partials. */
+int jr_sur_train_step(const JrSurrogate* sur, const float* descriptors, const double* energy_u,
+                      const int32_t* batch_idx, int32_t n_batch, int32_t n_atoms,
+                      float* params, float* adam_m, float* adam_v, int32_t step, float lr,
+                      float* loss, void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- measurement utility: FP32 FMA-pipe throughput probe ----
  * Launches n_blocks x 256 threads of independent FMA chains; *flops receives
  * the floating-point operations the launch performs (time it with events).

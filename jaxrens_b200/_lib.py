@@ -136,6 +136,21 @@ class JrInfoBuffers(C.Structure):
     ]
 
 
+SUR_BASIS, SUR_HIDDEN, SUR_PARAMS = 16, 64, 5313
+
+
+class JrSurrogate(C.Structure):
+    _fields_ = [
+        ("params", _vp),
+        ("in_scale", C.c_float * SUR_BASIS),
+        ("in_shift", C.c_float * SUR_BASIS),
+        ("out_scale", C.c_float),
+        ("out_shift", C.c_float),
+        ("contour_shift", C.c_float),
+        ("tau", C.c_float),
+    ]
+
+
 class JrLaunchConfig(C.Structure):
     _fields_ = [("threads", C.c_int32), ("tpa", C.c_int32), ("cluster", C.c_int32),
                 ("warp_walkers", C.c_int32)]
@@ -151,6 +166,9 @@ EXPORTED = (
     "jr_energy_forces",
     "jr_re_swap",
     "jr_autotune",
+    "jr_sur_descriptors",
+    "jr_sur_train_workspace_size",
+    "jr_sur_train_step",
     "jr_bench_fma_peak",
     "jr_last_error",
     "jr_version",
@@ -218,6 +236,15 @@ def load():
     L.jr_autotune.restype = C.c_int
     L.jr_autotune.argtypes = [
         P(JrDims), P(JrParams), P(JrStateBuffers), C.c_int32, P(JrLaunchConfig), _vp,
+    ]
+    L.jr_sur_descriptors.restype = C.c_int
+    L.jr_sur_descriptors.argtypes = [C.c_int32, C.c_int32, _vp, _vp, _vp, _vp]
+    L.jr_sur_train_workspace_size.restype = C.c_size_t
+    L.jr_sur_train_workspace_size.argtypes = [C.c_int32, C.c_int32]
+    L.jr_sur_train_step.restype = C.c_int
+    L.jr_sur_train_step.argtypes = [
+        P(JrSurrogate), _vp, _vp, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, C.c_int32,
+        C.c_float, _vp, _vp, C.c_size_t, _vp,
     ]
     L.jr_bench_fma_peak.restype = C.c_int
     L.jr_bench_fma_peak.argtypes = [C.c_int, C.c_int, _vp, C.POINTER(C.c_double), _vp]
