@@ -328,6 +328,48 @@ int jr_sur_train_step(const JrSurrogate* sur, const float* descriptors, const do
                       float* params, float* adam_m, float* adam_v, int32_t step, float lr,
                       float* loss, void* workspace, size_t workspace_bytes, void* stream);
 
+/* Surrogate energy (and forces) of a batch of single-species configurations,
+ * as the delayed-acceptance walk evaluates it: positions [B][Nmax][3], cell
+ * [B][9], n_atoms [B] (<= 64) on the device; energy_u [B] the surrogate U,
+ * forces [B][Nmax][3] = -dU/dx (may be NULL).  Radial pairs by the minimum
+ * image of the cell (periodic cells need sides > 7.6 A). */
+int jr_sur_energy_forces(const JrSurrogate* sur, int32_t n_configs, int32_t n_atoms_max,
+                         const float* positions, const float* cell, const int32_t* n_atoms,
+                         double* energy_u, float* forces, void* stream);
+
+/* Sample ring of the delayed-acceptance walk: every MWG step of every chain
+ * owns one slot, into which a step that evaluated the exact potential stores
+ * the evaluated configuration (positions, cell) and its model energy U; a
+ * step without an exact evaluation stores energy NaN.  Chain wi (0 = the
+ * clone, then the extras) of replica p in the launch's iteration it owns the
+ * T slots from base + ((it P + p) W + wi) T, modulo capacity (W = n_cull +
+ * n_extra, T = n_mcmc_steps); the caller advances base by n_iter P W T per
+ * launch.  Any pointer may be NULL (positions NULL: no recording). */
+typedef struct JrSampleRing {
+  float* positions;                  /* [capacity][Nmax][3] */
+  float* cell;                       /* [capacity][9] */
+  double* energy_u;                  /* [capacity] */
+  int64_t capacity;
+  int64_t base;
+  int32_t* n_surrogate_evaluations;  /* [n_iter][P][M] surrogate evaluations */
+} JrSampleRing;
+
+/* jr_ns_iterate for the Stillinger-Weber model (params.model.model ==
+ * JR_MODEL_SW, one species, walkers of <= 64 atoms, whole-CTA walkers of 512
+ * threads) with galilean and volume moves by two-stage delayed acceptance
+ * on the surrogate `sur`: stage 1 accepts with the ratio of the smoothed
+ * surrogate constraint sigmoid((emax + contour_shift - H_sur) / tau) (galilean
+ * trajectories reflect off the surrogate contour; volume moves also take the
+ * prior ratio and the cell checks), stage 2 evaluates the exact energy and
+ * accepts with 1{E' < emax} times the inverse ratio.  Other moves run as in
+ * jr_ns_iterate.  info.n_evaluations counts exact evaluations;
+ * ring->n_surrogate_evaluations the surrogate's.  `cfg` may be NULL (the
+ * heuristic shape). */
+int jr_ns_iterate_da(const JrDims* dims, const JrParams* params, const JrStateBuffers* state,
+                     const JrInfoBuffers* info, const JrSurrogate* sur,
+                     const JrSampleRing* ring, int32_t n_iter, const JrLaunchConfig* cfg,
+                     void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- measurement utility: FP32 FMA-pipe throughput probe ----
  * Launches n_blocks x 256 threads of independent FMA chains; *flops receives
  * the floating-point operations the launch performs (time it with events).

@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 # translation units linked into the one library (each is self-contained)
 SRCS = [os.path.join(CSRC, f) for f in ("jr_ns.cu", "jr_pair_ext.cu", "jr_pair_aux.cu", "jr_sw.cu",
-                                        "jr_sur.cu")]
+                                        "jr_sur.cu", "jr_swda.cu")]
 
 
 def _deps() -> list[str]:

@@ -151,6 +151,17 @@ class JrSurrogate(C.Structure):
     ]
 
 
+class JrSampleRing(C.Structure):
+    _fields_ = [
+        ("positions", _vp),
+        ("cell", _vp),
+        ("energy_u", _vp),
+        ("capacity", C.c_int64),
+        ("base", C.c_int64),
+        ("n_surrogate_evaluations", _vp),
+    ]
+
+
 class JrLaunchConfig(C.Structure):
     _fields_ = [("threads", C.c_int32), ("tpa", C.c_int32), ("cluster", C.c_int32),
                 ("warp_walkers", C.c_int32)]
@@ -169,6 +180,8 @@ EXPORTED = (
     "jr_sur_descriptors",
     "jr_sur_train_workspace_size",
     "jr_sur_train_step",
+    "jr_sur_energy_forces",
+    "jr_ns_iterate_da",
     "jr_bench_fma_peak",
     "jr_last_error",
     "jr_version",
@@ -245,6 +258,15 @@ def load():
     L.jr_sur_train_step.argtypes = [
         P(JrSurrogate), _vp, _vp, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, C.c_int32,
         C.c_float, _vp, _vp, C.c_size_t, _vp,
+    ]
+    L.jr_sur_energy_forces.restype = C.c_int
+    L.jr_sur_energy_forces.argtypes = [
+        P(JrSurrogate), C.c_int32, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp,
+    ]
+    L.jr_ns_iterate_da.restype = C.c_int
+    L.jr_ns_iterate_da.argtypes = [
+        P(JrDims), P(JrParams), P(JrStateBuffers), P(JrInfoBuffers), P(JrSurrogate),
+        P(JrSampleRing), C.c_int32, P(JrLaunchConfig), _vp, C.c_size_t, _vp,
     ]
     L.jr_bench_fma_peak.restype = C.c_int
     L.jr_bench_fma_peak.argtypes = [C.c_int, C.c_int, _vp, C.POINTER(C.c_double), _vp]

@@ -2,7 +2,8 @@
 // argument checks, launch-shape heuristics, shared-memory sizing and the
 // launch templates of each model family.  jr_ns.cu defines the shared state
 // (error text, attribute cache) and instantiates the pair family; jr_sw.cu
-// instantiates the Stillinger-Weber family.
+// instantiates the Stillinger-Weber family, jr_swda.cu its delayed-acceptance
+// walk.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -84,7 +85,7 @@ inline JrLaunchConfig ns_heuristic_config(const JrDims* d, int n_iter, int fam =
     c.warp_walkers = 0;
     // Stillinger-Weber: 512 threads (the pair scan and the triplet sides
     // spread over twice the lanes; measured 17% faster than 256 on 64 atoms)
-    c.threads = fam == jr::kFamSW ? 512 : (nmax <= 16 ? 128 : 256);
+    c.threads = jr::sw_family(fam) ? 512 : (nmax <= 16 ? 128 : 256);
     const int tpa = pow2_floor(c.threads / nmax);
     c.tpa = tpa > 16 ? 16 : (tpa < 1 ? 1 : tpa);
   }
@@ -158,7 +159,7 @@ inline int check_config(const JrLaunchConfig& c, const JrDims* d, int fam = jr::
   if (c.cluster < 1 || c.cluster > 16) return fail(JR_ERR_PARAM, "cluster must be in [1, 16]");
   if (c.warp_walkers != 0 && c.warp_walkers != 1)
     return fail(JR_ERR_PARAM, "warp_walkers must be 0 or 1");
-  if (c.warp_walkers && fam == jr::kFamSW)
+  if (c.warp_walkers && jr::sw_family(fam))
     return fail(JR_ERR_PARAM, "Stillinger-Weber walkers are walked by whole CTAs");
   if (!c.warp_walkers && c.tpa > c.threads) return fail(JR_ERR_PARAM, "tpa exceeds the CTA");
   if (c.warp_walkers && c.threads > 128)
@@ -173,8 +174,9 @@ inline int check_config(const JrLaunchConfig& c, const JrDims* d, int fam = jr::
   return JR_OK;
 }
 
-inline size_t ns_dyn_smem(const JrDims* d, const JrParams* p, const JrLaunchConfig& c) {
-  const int fam = family_of(p);
+inline size_t ns_dyn_smem(const JrDims* d, const JrParams* p, const JrLaunchConfig& c,
+                          int fam = -1) {
+  if (fam < 0) fam = family_of(p);
   const int cpc = c.warp_walkers ? c.threads / 32 : 1;
   return jr::dyn_head_bytes(d->n_walkers, d->n_atoms_max, p->model.n_images, d->n_cull, fam) +
          (size_t)cpc * jr::walker_smem_bytes(d->n_atoms_max, p->model.n_images, true, fam);
@@ -204,9 +206,9 @@ inline bool needs_ext_walk(const JrParams* p) {
 template <class G, int kT, bool kExt>
 int launch_ns_as(const JrDims* dims, const JrParams* params, const JrStateBuffers* state,
                  const JrInfoBuffers& inf, int n_iter, const JrLaunchConfig& c, void* workspace,
-                 cudaStream_t s) {
+                 cudaStream_t s, const jr::DaArgs& da) {
   auto kern = jr::ns_iterate_kernel<G, kT, kExt>;
-  const size_t smem = ns_dyn_smem(dims, params, c);
+  const size_t smem = ns_dyn_smem(dims, params, c, G::kFam);
   int rc = check_smem(smem);
   if (rc) return rc;
   cudaError_t e = ensure_attrs(reinterpret_cast<const void*>(kern), smem, c.cluster > 8);
@@ -224,7 +226,7 @@ int launch_ns_as(const JrDims* dims, const JrParams* params, const JrStateBuffer
   lc.attrs = attr;
   lc.numAttrs = 1;
   e = cudaLaunchKernelEx(&lc, kern, *dims, *params, *state, inf, n_iter, (int)c.tpa,
-                         (int)c.cluster, (const uint32_t*)workspace);
+                         (int)c.cluster, (const uint32_t*)workspace, da);
   if (e != cudaSuccess) return cuda_fail(e, "ns_iterate launch");
   return JR_OK;
 }
@@ -236,25 +238,27 @@ int launch_ns_as(const JrDims* dims, const JrParams* params, const JrStateBuffer
 template <int F, bool kExt>
 int launch_ns_walk(const JrDims* dims, const JrParams* params, const JrStateBuffers* state,
                    const JrInfoBuffers& inf, int n_iter, const JrLaunchConfig& c, void* workspace,
-                   cudaStream_t s) {
+                   cudaStream_t s, const jr::DaArgs& da) {
   using Cta = jr::CtaG<F>;
   if constexpr (F == jr::kFamPair) {
     if (c.warp_walkers)
       return launch_ns_as<jr::WarpG<F>, 128, kExt>(dims, params, state, inf, n_iter, c,
-                                                   workspace, s);
+                                                   workspace, s, da);
   }
-  if (c.threads <= 256)
-    return launch_ns_as<Cta, 256, kExt>(dims, params, state, inf, n_iter, c, workspace, s);
-  return launch_ns_as<Cta, 512, kExt>(dims, params, state, inf, n_iter, c, workspace, s);
+  if constexpr (F != jr::kFamSWDA) {
+    if (c.threads <= 256)
+      return launch_ns_as<Cta, 256, kExt>(dims, params, state, inf, n_iter, c, workspace, s, da);
+  }
+  return launch_ns_as<Cta, 512, kExt>(dims, params, state, inf, n_iter, c, workspace, s, da);
 }
 
 template <int F>
 int launch_ns_family(const JrDims* dims, const JrParams* params, const JrStateBuffers* state,
                      const JrInfoBuffers& inf, int n_iter, const JrLaunchConfig& c,
-                     void* workspace, cudaStream_t s) {
+                     void* workspace, cudaStream_t s, const jr::DaArgs& da) {
   if (needs_ext_walk(params))
-    return launch_ns_walk<F, true>(dims, params, state, inf, n_iter, c, workspace, s);
-  return launch_ns_walk<F, false>(dims, params, state, inf, n_iter, c, workspace, s);
+    return launch_ns_walk<F, true>(dims, params, state, inf, n_iter, c, workspace, s, da);
+  return launch_ns_walk<F, false>(dims, params, state, inf, n_iter, c, workspace, s, da);
 }
 
 // One move per (replica, trial) walker, model family F.
@@ -389,7 +393,7 @@ int launch_energy_family(const JrParams* params, int32_t n_configs, int32_t n_at
 // whole Stillinger-Weber family.
 #define JR_NS_WALK_ARGS                                                                      \
   const JrDims*, const JrParams*, const JrStateBuffers*, const JrInfoBuffers&, int,           \
-      const JrLaunchConfig&, void*, cudaStream_t
+      const JrLaunchConfig&, void*, cudaStream_t, const jr::DaArgs&
 #define JR_TRIAL_ARGS                                                                        \
   const JrDims*, const JrParams*, const JrStateBuffers*, int32_t, int32_t, const int32_t*,     \
       const uint32_t*, const uint32_t*, const float*, const double*, int32_t, int32_t*,       \
@@ -414,4 +418,7 @@ extern template int jrh::launch_ns_family<jr::kFamSW>(JR_NS_WALK_ARGS);
 extern template int jrh::launch_trial_family<jr::kFamSW>(JR_TRIAL_ARGS);
 extern template int jrh::launch_population_family<jr::kFamSW>(JR_POP_ARGS);
 extern template int jrh::launch_energy_family<jr::kFamSW>(JR_ENERGY_ARGS);
+#endif
+#ifndef JR_INSTANTIATE_SWDA
+extern template int jrh::launch_ns_family<jr::kFamSWDA>(JR_NS_WALK_ARGS);
 #endif

@@ -170,6 +170,14 @@ template <bool kExt, class G>
 __device__ __forceinline__ void walk_chain(const JrParams& P, Walker<G>& w, int T, Key chain_key,
                                   Key move_key, double emax, float pressure, const float* mu) {
   WalkShared& s = w.s;
+  if constexpr (G::kFam == kFamSWDA) {
+    // the surrogate energy of the loaded walker
+    double d0, d1;
+    const double ens = ensemble_term(s, s.cc[s.cur].vol, pressure, mu, P.model.n_species);
+    const double Hs = sur_ham<false>(w, s.cur, ens, d0, d1);
+    if (w.g.leader()) s.Esur = Hs;
+    w.g.sync();
+  }
   for (int t0 = 0; t0 < T; t0 += kStepChunk) {
     const int nt = T - t0 < kStepChunk ? T - t0 : kStepChunk;
     for (int q = w.g.rank(); q < nt; q += w.g.size()) {
@@ -197,8 +205,10 @@ __device__ __forceinline__ void walk_chain(const JrParams& P, Walker<G>& w, int 
       }
       w.g.sync();
     }
-    for (int t = 0; t < nt; ++t)
+    for (int t = 0; t < nt; ++t) {
+      w.ring_step = t0 + t;
       mwg_step<kExt>(P, w, s.step_key[t], s.step_move[t], emax, pressure, mu);
+    }
     w.g.sync();
   }
   {
@@ -517,11 +527,18 @@ __device__ inline void build_group_pair_table(const G& g, uint16_t* pij, int n) 
   g.sync();
 }
 
+// The surrogate and the sample ring of the delayed-acceptance walk (unused
+// by the other families).
+struct DaArgs {
+  JrSurrogate sur;
+  JrSampleRing ring;
+};
+
 template <class G, int kMaxThreads, bool kExt>
 __global__ void __launch_bounds__(kMaxThreads, 1)
 ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
                   const JrInfoBuffers info, const int n_iter, const int tpa, const int C,
-                  const uint32_t* __restrict__ key0_base) {
+                  const uint32_t* __restrict__ key0_base, const __grid_constant__ DaArgs da) {
   constexpr bool kWarp = G::kIsWarp;
   extern __shared__ __align__(16) unsigned char dyn[];
   __shared__ NsShared ns;
@@ -547,6 +564,17 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
   WalkShared* wsp = carve_walker(L.walkers + (size_t)my * L.walker_bytes, D.n_atoms_max, nimg,
                                  L.pij, arr, true, G::kFam);
   Walker<G> w{*wsp, arr, tab, n, tpa, make_group<G>(red), 0};
+  if constexpr (G::kFam == kFamSWDA) {
+    w.sur = &da.sur;
+    if (da.ring.positions) {
+      w.ring_pos = da.ring.positions;
+      w.ring_cell = da.ring.cell;
+      w.ring_u = da.ring.energy_u;
+      w.ring_nmax = D.n_atoms_max;
+      w.ring_cap = da.ring.capacity;
+    }
+    sur_load_weights(da.sur, arr);
+  }
   zero_pair_matrix(w.g, arr, D.n_atoms_max);
   int par = 0;
   __syncthreads();
@@ -631,6 +659,8 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
         const int dst = is_clone ? (ncull > 1 ? ns.cw[sidx] : ns.worst[0]) : src;
         if (is_clone) write_dead(w.g, D, st, info, committed, p, dst, n, sidx);
         load_walker(P, D, st, w, p, src, is_clone);
+        w.ring_chain = da.ring.base + ((long long)committed * D.n_replicas + p) * W * T +
+                       (long long)sidx * T;
         walk_chain<kExt>(P, w, T, split(ns.kmcmc[0], (uint32_t)sidx), ns.kmove[0], ns.e[0],
                          pressure, mu);
         store_walker(D, st, w, p, dst);
@@ -640,6 +670,8 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
       if (d < Dr && ns.spec[d]) {
         const int src = wi == 0 ? ns.clone[d] : ns.extras[d * nx + wi - 1];
         load_walker(P, D, st, w, p, src, wi == 0);
+        w.ring_chain = da.ring.base + ((long long)(committed + d) * D.n_replicas + p) * W * T +
+                       (long long)wi * T;
         walk_chain<kExt>(P, w, T, split(ns.kmcmc[d], (uint32_t)wi), ns.kmove[d], ns.e[d], pressure,
                          mu);
         if (w.g.leader()) ns.res_E[my] = w.s.E;
@@ -681,7 +713,7 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
         const int s0 = Dmax == 1 ? 0 : d_own * W;
         const int s1 = Dmax == 1 ? (slots < W ? slots : W) : d_own * W + W;
         for (int m = 0; m < M; ++m) {
-          int a = 0, pr = 0, ne = 0, ng = 0, rr[4] = {0, 0, 0, 0};
+          int a = 0, pr = 0, ne = 0, ng = 0, nsur = 0, rr[4] = {0, 0, 0, 0};
           for (int sl = s0; sl < s1; ++sl) {
             const WalkShared* local = reinterpret_cast<const WalkShared*>(
                 L.walkers + (size_t)(sl % cpc) * L.walker_bytes);
@@ -690,8 +722,10 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
             pr += rs->c_prop[m];
             ne += rs->c_nev[m];
             ng += rs->c_ngr[m];
+            nsur += rs->c_nsur[m];
             for (int q = 0; q < 4; ++q) rr[q] += rs->c_rr[4 * m + q];
           }
+          if (da.ring.n_surrogate_evaluations) da.ring.n_surrogate_evaluations[ib * M + m] = nsur;
           if (info.n_accepted) info.n_accepted[ib * M + m] = a;
           if (info.n_proposed) info.n_proposed[ib * M + m] = pr;
           if (info.n_evaluations) info.n_evaluations[ib * M + m] = ne;

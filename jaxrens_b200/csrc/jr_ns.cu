@@ -298,9 +298,12 @@ int jr_ns_iterate(const JrDims* dims, const JrParams* params, const JrStateBuffe
   cudaError_t e = cudaMemcpyAsync(workspace, ksrc, 2 * sizeof(uint32_t),
                                   cudaMemcpyDeviceToDevice, s);
   if (e != cudaSuccess) return cuda_fail(e, "key snapshot");
+  const jr::DaArgs none{};
   if (fam == jr::kFamSW)
-    return jrh::launch_ns_family<jr::kFamSW>(dims, params, state, inf, n_iter, c, workspace, s);
-  return jrh::launch_ns_family<jr::kFamPair>(dims, params, state, inf, n_iter, c, workspace, s);
+    return jrh::launch_ns_family<jr::kFamSW>(dims, params, state, inf, n_iter, c, workspace, s,
+                                             none);
+  return jrh::launch_ns_family<jr::kFamPair>(dims, params, state, inf, n_iter, c, workspace, s,
+                                             none);
 }
 
 }  // extern "C"

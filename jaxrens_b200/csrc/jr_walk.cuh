@@ -29,6 +29,11 @@ constexpr int kStepChunk = 64;  // steps whose keys and moves are drawn at once
 // stream.
 constexpr int kFamPair = 0;
 constexpr int kFamSW = 1;
+// Stillinger-Weber with the learned surrogate: galilean and volume moves by
+// two-stage delayed acceptance, the exact SW energy deciding every step
+constexpr int kFamSWDA = 2;
+
+__host__ __device__ constexpr bool sw_family(int fam) { return fam == kFamSW || fam == kFamSWDA; }
 
 // The key of one MWG step with its two first-level subkeys, split(k, 0) and
 // split(k, 1), which every move draws from (galilean: initial direction and
@@ -175,6 +180,11 @@ struct WalkShared {
   double E_save;
   int cur_save;
   int counts_save[JR_MAX_SPECIES];
+  // surrogate walk: the surrogate potential (with the ensemble term) of the
+  // current walker, and the exact / surrogate evaluations of the last move
+  double Esur;
+  int step_nev, step_nsur;
+  int c_nsur[JR_MAX_MOVES];  // per-chain surrogate evaluations per move
 };
 
 // Pair tables of the model, shared by every walker of a CTA.
@@ -208,7 +218,29 @@ struct WalkArrays {
   uint64_t* nbm;        // [2][kSWMaxAtoms] neighbour masks (alternating evaluations)
   uint16_t* cand;       // [kSWCandDense + n(n-1)/2] pairs inside the cutoff: per-warp
                         // segments, then (from kSWCandDense) the dense list
+  // surrogate network (the SW-with-surrogate family only): bfloat16 operand
+  // tiles of the warp-level products, row-major with padded rows
+  uint16_t* sw1t;       // [64][kSurLdX]   W1^T (n = hidden, k = input)
+  uint16_t* sw2t;       // [64][kSurLdH]   W2^T (n = out, k = in)
+  uint16_t* sw2k;       // [64][kSurLdH]   W2   (n = in, k = out)
+  uint16_t* sw1k;       // [16][kSurLdH]   W1   (n = input, k = hidden)
+  uint16_t* sx;         // [64][kSurLdX]   network input rows
+  uint16_t* sh1;        // [64][kSurLdH]   first hidden layer
+  uint16_t* sg2;        // [64][kSurLdH]   gradient at the second layer
+  uint16_t* sg1;        // [64][kSurLdH]   gradient at the first layer
+  float* sbias;         // [3][64] b1, b2, w3
+  float* sdx;           // [64][16] gradient of the energy at the inputs
+  float* separt;        // [4][64] per-row energy partials of the column groups
 };
+
+// Padded row strides (bfloat16 elements) of the surrogate's operand tiles:
+// the warp-level fragment loads of 8 rows x 4 columns fall on distinct banks.
+constexpr int kSurLdX = 24, kSurLdH = 72;
+
+__host__ __device__ inline size_t sur_table_bytes() {
+  return 2u * (64u * kSurLdX * 2u + 64u * kSurLdH * 5u + 16u * kSurLdH) + 4u * (3u * 64u) +
+         4u * (64u * 16u) + 4u * (4u * 64u);
+}
 
 __host__ __device__ inline bool use_pair_matrix(int nmax, int nimg, int fam = kFamPair) {
   return fam == kFamPair && nimg == 1 && nmax <= kPairMatMax;
@@ -247,7 +279,8 @@ __host__ __device__ inline size_t walker_smem_bytes(int nmax, int nimg, bool nor
   b += 2u * 16u * (size_t)nmax + 4u * 12u * (size_t)nmax;
   b += align16(2u * 3u * 4u * (size_t)nimg);
   if (use_pair_matrix(nmax, nimg, fam)) b += align16(12u * (size_t)nmax * (size_t)pm_stride(nmax));
-  if (fam == kFamSW) b += sw_table_bytes(nmax);
+  if (sw_family(fam)) b += sw_table_bytes(nmax);
+  if (fam == kFamSWDA) b += align16(sur_table_bytes());
   if (use_normal_buffer(nmax, normals)) b += align16(12u * (size_t)kStepChunk * (size_t)nmax);
   return align16(b);
 }
@@ -255,7 +288,7 @@ __host__ __device__ inline size_t walker_smem_bytes(int nmax, int nimg, bool nor
 // Bytes of the CTA-shared pair decode table (the pair-matrix path and every
 // Stillinger-Weber walk).
 __host__ __device__ inline size_t pair_table_bytes(int nmax, int nimg, int fam = kFamPair) {
-  return (use_pair_matrix(nmax, nimg, fam) || fam == kFamSW) ? align16(2u * pair_count(nmax)) : 0;
+  return (use_pair_matrix(nmax, nimg, fam) || sw_family(fam)) ? align16(2u * pair_count(nmax)) : 0;
 }
 
 __device__ inline WalkShared* carve_walker(char* p, int nmax, int nimg, const uint16_t* pij,
@@ -275,12 +308,14 @@ __device__ inline WalkShared* carve_walker(char* p, int nmax, int nimg, const ui
   a.swr0 = a.swr1 = a.swq = nullptr;
   a.nbm = nullptr;
   a.cand = nullptr;
+  a.sw1t = a.sw2t = a.sw2k = a.sw1k = a.sx = a.sh1 = a.sg2 = a.sg1 = nullptr;
+  a.sbias = a.sdx = a.separt = nullptr;
   if (use_pair_matrix(nmax, nimg, fam)) {
     a.pm = (float*)p;
     a.pij = pij;
     p += align16(12u * (size_t)nmax * (size_t)pm_stride(nmax));
   }
-  if (fam == kFamSW) {
+  if (sw_family(fam)) {
     const size_t np = pair_count(nmax);
     a.pij = pij;
     a.swr0 = (float4*)p; p += 16u * np;
@@ -288,6 +323,21 @@ __device__ inline WalkShared* carve_walker(char* p, int nmax, int nimg, const ui
     a.swq = (float4*)p; p += 16u * np;
     a.nbm = (uint64_t*)p; p += 2u * 8u * kSWMaxAtoms;
     a.cand = (uint16_t*)p; p += align16(2u * ((size_t)kSWCandDense + np));
+  }
+  if (fam == kFamSWDA) {
+    char* q = p;
+    a.sw1t = (uint16_t*)q; q += 2 * 64 * kSurLdX;
+    a.sx = (uint16_t*)q; q += 2 * 64 * kSurLdX;
+    a.sw2t = (uint16_t*)q; q += 2 * 64 * kSurLdH;
+    a.sw2k = (uint16_t*)q; q += 2 * 64 * kSurLdH;
+    a.sh1 = (uint16_t*)q; q += 2 * 64 * kSurLdH;
+    a.sg2 = (uint16_t*)q; q += 2 * 64 * kSurLdH;
+    a.sg1 = (uint16_t*)q; q += 2 * 64 * kSurLdH;
+    a.sw1k = (uint16_t*)q; q += 2 * 16 * kSurLdH;
+    a.sbias = (float*)q; q += 4 * 3 * 64;
+    a.sdx = (float*)q; q += 4 * 64 * 16;
+    a.separt = (float*)q; q += 4 * 4 * 64;
+    p += align16(sur_table_bytes());
   }
   a.nz = use_normal_buffer(nmax, normals) ? (float*)p : nullptr;
   return s;
@@ -335,6 +385,18 @@ struct Walker {
   // pairs (LJ: unique interactions; Stillinger-Weber: pairs inside the
   // cutoff) and triplets, with forces, then energy-only
   int tc[4] = {0, 0, 0, 0};
+  // sample ring of exactly evaluated configurations (recording when
+  // ring_pos is set): step t of the chain owns slot (ring_chain + t) mod
+  // ring_cap; ring_step is the current step (every thread's copy)
+  float* ring_pos = nullptr;   // [cap][Nmax][3]
+  float* ring_cell = nullptr;  // [cap][9]
+  double* ring_u = nullptr;    // [cap] model energy U, NaN: slot holds no evaluation
+  int ring_nmax = 0;
+  long long ring_cap = 0;
+  long long ring_chain = 0;
+  int ring_step = 0;
+  // surrogate walk: the CTA's copy of the surrogate's scalars
+  const JrSurrogate* sur = nullptr;
 };
 
 __device__ __forceinline__ float& pos_at(float4* xs, int idx) {
@@ -908,7 +970,7 @@ __device__ __forceinline__ void model_eval_pair(const JrParams& P, Walker<G>& w,
 template <bool kForces, class G>
 __device__ __forceinline__ void model_eval(const JrParams& P, Walker<G>& w, int cidx, double& U, double& sff,
                            double& sfd) {
-  if constexpr (G::kFam == kFamSW) {
+  if constexpr (sw_family(G::kFam)) {
     const CellCtx& ccs = w.s.cc[cidx];
     if (ccs.diag) sw_eval<kForces, true>(P, w, load_mic<true>(ccs), U, sff, sfd);
     else sw_eval<kForces, false>(P, w, load_mic<false>(ccs), U, sff, sfd);
@@ -1051,7 +1113,7 @@ __device__ __forceinline__ bool move_galilean(const JrParams& P, Walker<G>& w, c
   const double E0 = w.s.E;
   double E;
   const JrModelParams& mp = P.model;
-  if constexpr (G::kFam == kFamSW) {
+  if constexpr (sw_family(G::kFam)) {
     const double ens = ensemble_term(w.s, w.s.cc[w.s.cur].vol, pressure, mu, mp.n_species);
     if (w.s.cc[w.s.cur].diag) E = galilean_trajectory<kTrajSW, true, true>(P, w, step, R, emax, ens);
     else E = galilean_trajectory<kTrajSW, true, false>(P, w, step, R, emax, ens);
@@ -1419,12 +1481,27 @@ __device__ __forceinline__ bool move_swap(const JrParams& P, Walker<G>& w, const
   return acc;
 }
 
+}  // namespace jr
+
+#include "jr_da.cuh"
+
+namespace jr {
+
 // One move of type P.moves.type[idx]; returns acceptance and reject reason.
+// The surrogate family walks its galilean and volume moves by delayed
+// acceptance.
 template <class G>
 __device__ __forceinline__ bool run_move(const JrParams& P, Walker<G>& w, int idx, const StepKey& key,
                                          float step, double emax, float pressure,
                                          const float* mu, int& reason) {
   reason = 0;
+  if constexpr (G::kFam == kFamSWDA) {
+    if (P.moves.type[idx] == JR_MOVE_GALILEAN)
+      return da_galilean(P, w, key, step, P.moves.n_reflect[idx], P.moves.perturb_angle[idx],
+                         emax, pressure, mu, reason);
+    if (P.moves.type[idx] == JR_MOVE_VOLUME)
+      return da_volume(P, w, key, step, emax, pressure, mu, reason);
+  }
   switch (P.moves.type[idx]) {
     case JR_MOVE_GALILEAN:
       return move_galilean(P, w, key, step, P.moves.n_reflect[idx], P.moves.perturb_angle[idx],
@@ -1545,8 +1622,38 @@ __device__ __forceinline__ void mwg_step(const JrParams& P, Walker<G>& w, const 
                                          double emax, float pressure, const float* mu) {
   WalkShared& s = w.s;
   int reason = 0;
+  if (G::kFam == kFamSWDA && w.g.leader()) {
+    s.step_nev = 1;
+    s.step_nsur = 0;
+  }
   const bool acc = gated_move<kExt>(P, w, idx, step_key, s.step_sizes[idx], emax, pressure, mu,
                                    reason);
+  if constexpr (G::kFam == kFamSWDA) {
+    const int ty = P.moves.type[idx];
+    if ((ty != JR_MOVE_GALILEAN && ty != JR_MOVE_VOLUME) || reason == 4) {
+      // another move (or the constraint gate's undo) changed the walker: its
+      // surrogate energy anew
+      double d0, d1;
+      const double ens = ensemble_term(s, s.cc[s.cur].vol, pressure, mu, P.model.n_species);
+      const double Hs = sur_ham<false>(w, s.cur, ens, d0, d1);
+      if (w.g.leader()) s.Esur = Hs;
+    }
+    if (w.g.leader()) {
+      // the step's ring slot holds no exact evaluation
+      if (w.ring_pos && ((ty != JR_MOVE_GALILEAN && ty != JR_MOVE_VOLUME) || s.step_nev == 0))
+        w.ring_u[(w.ring_chain + w.ring_step) % w.ring_cap] = __longlong_as_double(
+            0x7ff8000000000000ll);
+      s.c_prop[idx] += 1;
+      s.c_nsur[idx] += s.step_nsur;
+      s.c_nev[idx] += s.step_nev;
+      s.w_prop[idx] += 1;
+      s.w_acc[idx] += acc ? 1 : 0;
+      s.c_acc[idx] += acc ? 1 : 0;
+      const int col = acc ? 0 : (reason > 1 ? reason : 1);
+      if (col < 4) s.c_rr[idx * 4 + col] += 1;
+    }
+    return;
+  }
   if (w.g.leader()) {
     s.w_prop[idx] += 1;
     s.w_acc[idx] += acc ? 1 : 0;
@@ -1650,7 +1757,7 @@ __device__ __forceinline__ void store_walker(const JrDims& D, const JrStateBuffe
 __device__ inline void zero_chain_counters(WalkShared& s) {
   for (int q = 0; q < 4; ++q) s.c_terms[q] = 0;
   for (int m = 0; m < JR_MAX_MOVES; ++m) {
-    s.c_acc[m] = s.c_prop[m] = s.c_nev[m] = s.c_ngr[m] = 0;
+    s.c_acc[m] = s.c_prop[m] = s.c_nev[m] = s.c_ngr[m] = s.c_nsur[m] = 0;
     s.c_rr[4 * m] = s.c_rr[4 * m + 1] = s.c_rr[4 * m + 2] = s.c_rr[4 * m + 3] = 0;
   }
 }
