@@ -533,10 +533,13 @@ __device__ __forceinline__ bool da_volume(const JrParams& P, Walker<G>& w, const
   const double Hs0 = s.Esur;
   const float ls1 = sur_log_s(Hs1, contour, S.tau), ls0 = sur_log_s(Hs0, contour, S.tau);
   // log of min(1, ratio^N) (flat prior: 0)
-  const float lprior = mv.flat_v_prior ? 0.0f : fminf(0.0f, (float)n * logf(ratio));
+  const double pa = volume_prior(ratio, n, mv.flat_v_prior != 0);
   const bool valid = s.cell_ok != 0;
   const float u1 = key.pre ? key.vu : uniform01(bits32(key.k1, 0u));
-  const bool stage1 = valid && logf(u1) < fminf(0.0f, lprior + ls1 - ls0);
+  // u1 < min(1, pa s(x') / s(x)); a flat surrogate constraint leaves the
+  // prior test of the exact move
+  const double r1 = pa * exp((double)ls1 - (double)ls0);
+  const bool stage1 = valid && (double)u1 < (r1 < 1.0 ? r1 : 1.0);
   bool acc = false;
   double En = s.E;
   int nev = 0;

@@ -1179,6 +1179,24 @@ __device__ inline bool cell_valid(const float* c, int n, const JrMoveParams& mv)
   return (vpa <= mv.max_vpa) && (vpa >= mv.min_vpa) && (amin >= mv.min_aspect);
 }
 
+// Acceptance probability of the volume prior: 1 for a flat prior, else
+// min(1, ratio**N) by lax.integer_pow's binary exponentiation, in float64.
+__device__ __forceinline__ double volume_prior(float ratio, int n, bool flat) {
+  if (flat) return 1.0;
+  double acc = 1.0, b = (double)ratio;
+  bool first = true;
+  int y = n;
+  while (y > 0) {
+    if (y & 1) {
+      acc = first ? b : acc * b;
+      first = false;
+    }
+    y >>= 1;
+    if (y > 0) b = b * b;
+  }
+  return acc < 1.0 ? acc : 1.0;
+}
+
 // Volume move (volume.py:49-109 + _common.py:16-93).  Returns acceptance and
 // the reject reason (priority energy > cell > prior).
 template <class G>
@@ -1216,25 +1234,7 @@ __device__ __forceinline__ bool move_volume(const JrParams& P, Walker<G>& w, con
   const double En = ham_eval<false>(P, w, tr, pressure, mu, d0, d1);
   const bool valid = s.cell_ok != 0;
   const float u = key.pre ? key.vu : uniform01(bits32(k2, 0u));
-  bool prior_ok;
-  if (mv.flat_v_prior) {
-    prior_ok = u < 1.0f;
-  } else {
-    // min(1, ratio**N): lax.integer_pow's binary exponentiation, in float64
-    double acc = 1.0, b = (double)ratio;
-    bool first = true;
-    int y = n;
-    while (y > 0) {
-      if (y & 1) {
-        acc = first ? b : acc * b;
-        first = false;
-      }
-      y >>= 1;
-      if (y > 0) b = b * b;
-    }
-    const double pa = acc < 1.0 ? acc : 1.0;
-    prior_ok = (double)u < pa;
-  }
+  const bool prior_ok = (double)u < volume_prior(ratio, n, mv.flat_v_prior != 0);
   const bool energy_ok = En < emax;
   const bool acc = energy_ok && valid && prior_ok;
   reason = acc ? 0 : (!energy_ok ? 1 : (!valid ? 2 : 3));
