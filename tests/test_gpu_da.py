@@ -8,7 +8,7 @@
   two-stage moves to the exact ones: with one-step galilean trajectories the
   walk is the plain walk, walker for walker and bit for bit;
 - invariants of a walk with an untrained surrogate: every stored energy is
-  the exact potential of its walker, the contour rises, every walker sits
+  the exact potential of its walker, the contour falls, every walker sits
   below it, the sample ring holds exactly the configurations the walk
   evaluated with their exact energies, and the counters add up (one exact
   evaluation per galilean or volume step at most, n_reflect or more
@@ -140,9 +140,9 @@ def test_walk_with_untrained_surrogate_keeps_the_exact_invariants():
     vol = np.abs(np.linalg.det(c.astype(np.float64)))
     e64 = _np(pop.energy64)
     np.testing.assert_allclose(e64, U + np.float32(P_SI) * vol.astype(np.float32), rtol=1e-6)
-    # the contour rises and every walker sits below the last one
+    # the contour falls and every walker sits below the last one
     dead = _np(info.dead_energy)
-    assert (np.diff(dead, axis=0) >= 0).all()
+    assert (np.diff(dead, axis=0) <= 0).all()
     assert (e64 < dead[-1][:, None]).all()
     # counters per move (0 galilean, 1 volume)
     prop, ne = _np(info.n_proposed), _np(info.n_evaluations)
