@@ -89,7 +89,7 @@ def select_workload(name: str) -> None:
         desc = ("binary LJ semi-grand (Kob-Andersen pair tables), 16 runs with N in "
                 "{16..96} x 1024 walkers, Delta-mu in [-2, 2], n_mcmc_steps=40, "
                 "galilean(n_reflect=10)+volume+morph+swap")
-    elif name == "sw":
+    elif name in ("sw", "sw_da"):
         from jaxrens_b200.backends import EV_PER_A3_PER_GPA
 
         P_RUNS, K, N, T = 4, 1024, 64, 40
@@ -99,6 +99,12 @@ def select_workload(name: str) -> None:
         STEP_SIZES = (0.2, 2.8)
         desc = ("Stillinger-Weber Si-64 NPT, 4 runs at 0.1 GPa x 1024 walkers, "
                 "n_mcmc_steps=40, galilean(n_reflect=10)+volume")
+        if name == "sw_da":
+            STEP_SIZES = (0.05, 0.5)
+            desc = ("Stillinger-Weber Si-64 NPT, 4 runs at 0.1 GPa x 1024 walkers, "
+                    "n_mcmc_steps=40, galilean(n_reflect=10, 0.05 A)+volume(0.5 A^3/atom), "
+                    "condensed start: diamond cells scaled by up to +-6% in volume, "
+                    "atoms displaced uniformly by up to 0.35 A")
     else:
         raise SystemExit(f"unknown workload {name}")
     CONFIG = {"workload": desc, "n_runs": P_RUNS, "n_walkers": K,
@@ -116,6 +122,25 @@ FLOPS_EF, FLOPS_E = 61.0, 48.0
 SW_FLOPS = (74.0, 60.0, 58.0, 12.0)
 
 
+def condensed_silicon(seed: int, count: int, amp: float = 0.35):
+    """``count`` 64-atom silicon cells (2x2x2 conventional diamond cells,
+    a = 5.431 A) scaled by (1 + U(-0.06, 0.06))^(1/3) and with every atom
+    displaced by U(-amp, amp) A per coordinate: the solid-like walkers of a
+    late nested-sampling run (numpy-seeded synthetic data)."""
+    rng = np.random.default_rng(seed)
+    basis = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0], [.25, .25, .25],
+                      [.25, .75, .75], [.75, .25, .75], [.75, .75, .25]])
+    cells = np.array([[i, j, k] for i in range(2) for j in range(2) for k in range(2)])
+    x0 = ((cells[:, None, :] + basis[None]).reshape(-1, 3) * 5.431)
+    c0 = np.eye(3) * 2 * 5.431
+    pos, cel = [], []
+    for _ in range(count):
+        f = (1.0 + rng.uniform(-0.06, 0.06)) ** (1.0 / 3.0)
+        pos.append(x0 * f + rng.uniform(-amp, amp, x0.shape))
+        cel.append(c0 * f)
+    return np.asarray(pos, np.float32), np.asarray(cel, np.float32)
+
+
 def build_case(seed: int):
     from jaxrens_b200 import EnsembleTerm, Hamiltonian, build_mwg, create_lj, create_sw, prng
     from jaxrens_b200 import init as jinit
@@ -124,7 +149,7 @@ def build_case(seed: int):
     if WORKLOAD == "uneven":
         model = create_lj(epsilon=[[1.0, 1.5], [1.5, 0.5]], sigma=[[1.0, 0.8], [0.8, 0.88]],
                           cutoff=2.5)
-    elif WORKLOAD == "sw":
+    elif WORKLOAD in ("sw", "sw_da"):
         model = create_sw()
     else:
         model = create_lj(epsilon=1.0, sigma=1.0, cutoff=2.5)
@@ -138,7 +163,10 @@ def build_case(seed: int):
     keys = prng.split(root, P_RUNS + 3)
     pos, cells = [], []
     for r in range(P_RUNS):
-        p_, c_ = jinit.uniform_gas(keys[r], K, N_LIST[r], V_PER_ATOM * N_LIST[r])
+        if WORKLOAD == "sw_da":
+            p_, c_ = condensed_silicon(seed * 1000 + r, K)
+        else:
+            p_, c_ = jinit.uniform_gas(keys[r], K, N_LIST[r], V_PER_ATOM * N_LIST[r])
         pos.append(p_)
         cells.append(c_)
     if WORKLOAD == "uneven":
@@ -286,7 +314,7 @@ def run_ours(args):
         if RE_ON:
             re.apply(ns, step)
     torch.cuda.synchronize()
-    if args.tune:
+    if args.tune and cfg is None:
         # tuned on the walkers past the prologue, the state the timed steps see
         best = _lib.JrLaunchConfig()
         dims = nsm.make_dims(ns, step, T, 0)
@@ -600,6 +628,128 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def _da_arm(name, ns, step, n_steps, walk, torch):
+    """Time n_steps steps of RE_INTERVAL iterations of ``walk(ns)`` (which
+    returns the step's info buffers), with an L2 flush between steps; the
+    counters summed over the steps."""
+    dev = ns.rng_key.device
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(n_steps)]
+    M = step.n_moves
+    acc = torch.zeros(M, dtype=torch.float64, device=dev)
+    prop = torch.zeros(M, dtype=torch.float64, device=dev)
+    nev = torch.zeros(M, dtype=torch.float64, device=dev)
+    nsur = torch.zeros(M, dtype=torch.float64, device=dev)
+    for k in range(n_steps):
+        flush.fill_(float(k))
+        ev[k][0].record()
+        info = walk(ns)
+        ev[k][1].record()
+        acc += info.n_accepted.sum(dim=(0, 1), dtype=torch.float64)
+        prop += info.n_proposed.sum(dim=(0, 1), dtype=torch.float64)
+        nev += info.n_evaluations.sum(dim=(0, 1), dtype=torch.float64)
+        if getattr(info, "n_surrogate_evaluations", None) is not None:
+            nsur += info.n_surrogate_evaluations.sum(dim=(0, 1), dtype=torch.float64)
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    ws = n_steps * RE_INTERVAL * P_RUNS * T
+    return {"arm": name, "value": ws / (ms * 1e-3), "ms_per_step": ms / n_steps,
+            "accepted_steps_per_s": float(acc.sum()) / (ms * 1e-3),
+            "acceptance_per_move": (acc / prop).tolist(),
+            "exact_evaluations_per_walker_step": float(nev.sum()) / ws,
+            "exact_evaluations_per_move_step": (nev / prop).tolist(),
+            "surrogate_evaluations_per_walker_step": float(nsur.sum()) / ws}
+
+
+def run_da(args):
+    """The Stillinger-Weber workload walked by delayed acceptance on the
+    learned surrogate, beside the exact walk from the same state.  After the
+    (exact, untimed) prologue the surrogate is bootstrapped from the live
+    walkers and the prologue's dead walkers; the timed DA steps include the
+    online training (16 Adam steps of 256 ring samples every 200 iterations)
+    and its recalibration.  Arms: da (trained), da_untrained (normalisation
+    only), exact."""
+    import torch
+
+    from jaxrens_b200 import delayed_acceptance as da
+    from jaxrens_b200 import nested_sampling as nsm
+    from jaxrens_b200.surrogate import Surrogate
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(0)
+    H, init_fn, step, pos, cells, types, run_keys, _ = build_case(args.seed)
+    ns = nsm.init_ns_parallel(init_fn, pos, types, None, cells, run_keys,
+                              ensemble_params={"pressure": PRESSURES})
+    info = nsm.InfoBuffers(ns, step.n_moves, RE_INTERVAL, dead=True)
+    dx, dc = [], []
+    for _ in range(args.prologue // RE_INTERVAL):
+        nsm.ns_iterate(ns, step, RE_INTERVAL, T, 0, info=info)
+        dx.append(info.dead_positions.reshape(-1, N, 3).clone())
+        dc.append(info.dead_cell.reshape(-1, 3, 3).clone())
+    torch.cuda.synchronize()
+    ns_exact, ns_untr = ns.clone(), ns.clone()
+    drv = da.DelayedAcceptanceNS(ns, step, n_mcmc_steps=T, ring_capacity=100_000,
+                                 train_every=200, train_steps=16, batch=256, lr=1e-3,
+                                 bootstrap_steps=600, seed=args.seed)
+    t0 = time.time()
+    drv.bootstrap(torch.cat(dx) if dx else None, torch.cat(dc) if dc else None)
+    torch.cuda.synchronize()
+    boot_s = time.time() - t0
+    untr = Surrogate(seed=args.seed + 1)
+    untr.in_scale, untr.in_shift = drv.sur.in_scale, drv.sur.in_shift
+    untr.out_scale, untr.out_shift = drv.sur.out_scale, drv.sur.out_shift
+    untr.tau, untr.contour_shift = drv.sur.tau, drv.sur.contour_shift
+
+    def walk_da(s):
+        out = drv.run(RE_INTERVAL, block=RE_INTERVAL)
+        return out
+
+    def walk_untr(s):
+        return da.ns_iterate_da(s, step, untr, RE_INTERVAL, T)
+
+    def walk_exact(s):
+        return nsm.ns_iterate(s, step, RE_INTERVAL, T, 0)
+
+    for _ in range(args.warmup):
+        walk_da(ns)
+        walk_untr(ns_untr)
+        walk_exact(ns_exact)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    arms = [_da_arm("da", ns, step, args.steps, walk_da, torch),
+            _da_arm("da_untrained", ns_untr, step, args.steps, walk_untr, torch),
+            _da_arm("exact", ns_exact, step, args.steps, walk_exact, torch)]
+    clk = clocks.stop()
+    # one training round on its own (16 Adam steps and the recalibration)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record()
+    drv.train(drv.train_steps)
+    t1.record()
+    torch.cuda.synchronize()
+    train_ms = t0.elapsed_time(t1)
+    line = {
+        "metric": METRIC, "value": arms[0]["value"], "unit": "walker-steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": arms[0]["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 SW terms, bf16 surrogate products with f32 accumulation",
+        "data": "synthetic", "config": dict(CONFIG, walk="delayed acceptance"),
+        "l2": "flushed (256 MiB write) between timed steps",
+        "surrogate": {"bootstrap_s": boot_s, "train_round_ms": train_ms,
+                      "train_every_iterations": drv.train_every,
+                      "contour_shift": drv.sur.contour_shift,
+                      "tau": drv.sur.tau, "ring_samples": drv.ring.reserved},
+        "arms": arms,
+        "da_over_exact": arms[0]["value"] / arms[2]["value"],
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -619,7 +769,7 @@ def main():
     ap.add_argument("--tpa", type=int, default=8)
     ap.add_argument("--warp", type=int, default=0)
     ap.add_argument("--workload", default="batched",
-                    choices=["batched", "single", "uneven", "sw"],
+                    choices=["batched", "single", "uneven", "sw", "sw_da"],
                     help="batched (default, the headline line), or the single-run, uneven "
                          "semi-grand and Stillinger-Weber configurations")
     args = ap.parse_args()
@@ -630,6 +780,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "sw_da":
+        run_da(args)
     else:
         run_ours(args)
 

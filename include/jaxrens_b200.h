@@ -331,7 +331,8 @@ int jr_sur_train_step(const JrSurrogate* sur, const float* descriptors, const do
 /* Surrogate energy (and forces) of a batch of single-species configurations,
  * as the delayed-acceptance walk evaluates it: positions [B][Nmax][3], cell
  * [B][9], n_atoms [B] (<= 64) on the device; energy_u [B] the surrogate U,
- * forces [B][Nmax][3] = -dU/dx (may be NULL).  Radial pairs by the minimum
+ * forces [B][Nmax][3] = -dU/dx (NULL: the energy alone, as the walk's
+ * trajectory steps evaluate it).  Radial pairs by the minimum
  * image of the cell (periodic cells need sides > 7.6 A). */
 int jr_sur_energy_forces(const JrSurrogate* sur, int32_t n_configs, int32_t n_atoms_max,
                          const float* positions, const float* cell, const int32_t* n_atoms,

@@ -3,18 +3,18 @@
 // (jr_sur.cuh) evaluated inside the walk on the walker resident in shared
 // memory, and the galilean and volume moves in two stages.
 //
-// Surrogate evaluation, one walker (n <= 64 atoms) on a 512-thread CTA:
-//   1. pair scan within the descriptor cutoff (minimum image, r^2), compacted
-//      in per-warp segments, with the neighbour masks; 2. per pair r and the
-//      cosine cutoff; 3. descriptors, thread (atom i, basis pair k) summing
-//      its neighbours in ascending order, standardised and rounded to
-//      bfloat16; 4. the two hidden layers as warp-level tensor-core products
-//      (mma.sync m16n8k16, bfloat16 operands, float32 accumulation; warp w
-//      owns rows 16 (w / 4).. and columns 16 (w % 4)..), SiLU, per-row
-//      energies; 5. with forces only: the backward products, dU/dD, the pair
-//      force coefficients sum_k (dU/dD_ik + dU/dD_jk) dphi_k(r) / r and the
-//      per-atom gather of the Stillinger-Weber path.
-//
+// Surrogate evaluation, one walker (n <= 64 atoms) on a 512-thread CTA, no
+// pair list: 1. descriptors, eight threads per atom, each over every eighth
+// other atom (minimum image, r^2 test, the 16 basis values by a two-exponential
+// product recurrence), summed over the eight threads, standardised and
+// rounded to bfloat16; 2.-3. the two hidden layers as warp-level tensor-core
+// products (mma.sync m16n8k16, bfloat16 operands, float32 accumulation; warp
+// w owns rows 16 (w / 4).. and columns 16 (w % 4)..; the four warps of a row
+// tile meet at a named barrier), SiLU, the energy; 4. with forces only: the
+// backward products down to dU/dD; 5. each atom's force from its neighbours
+// (both sides of every pair evaluated, so no scatter), summed over its eight
+// threads.
+
 // Delayed acceptance (J. A. Christen and C. Fox, J. Comput. Graph. Stat. 14,
 // 795 (2005)) with the smoothed surrogate constraint
 //   s(x) = sigmoid((emax + contour_shift - H_sur(x)) / tau),
@@ -81,112 +81,115 @@ __device__ inline void sur_load_weights(const JrSurrogate& S, const WalkArrays& 
   }
 }
 
+// Barrier of the 4 warps (128 threads) that own row tile `grp` of the
+// surrogate's products (named barriers 1..4; barrier 0 is the CTA's).
+__device__ __forceinline__ void rows_sync(int grp) {
+  asm volatile("bar.sync %0, 128;" ::"r"(grp + 1) : "memory");
+}
+
+// The 16 radial basis values g_k = exp(-(t - k)^2 / 2), t = (r - mu_0) / dmu,
+// scaled by e^60, by a product recurrence from k = 0 (two exponentials per
+// distance): g'_0 = exp(60 - t^2 / 2), g'_{k+1} = g'_k R_k with R_0 =
+// exp(t - 1/2) and R_{k+1} = R_k / e.  The scale keeps every value a normal
+// float for the distances inside the cutoff (t in [-9.8, 15]: g'_k between
+// about e^-53 and e^60); callers fold e^-60 into the cutoff factor.
+constexpr float kSurGScale = 8.75651076269652e-27f;  // e^-60
+
+__device__ __forceinline__ void sur_gauss16(float t, float* g) {
+  constexpr float kInvE = 0.36787944117144233f;
+  float h = __expf(60.0f - 0.5f * t * t);
+  float R = __expf(t - 0.5f);
+  g[0] = h;
+#pragma unroll
+  for (int k = 1; k < 16; ++k) {
+    h *= R;
+    R *= kInvE;
+    g[k] = h;
+  }
+}
+
+// Sum v[0..15] over the 8 lanes sub = lane & 7 of an aligned group
+// (reduce-scatter: 14 shuffles); lane sub ends with the totals of entries
+// 2 sub and 2 sub + 1 in v[0], v[1].
+__device__ __forceinline__ void sum16_over8(float* v, int sub) {
+  const bool h4 = (sub & 4) != 0, h2 = (sub & 2) != 0, h1 = (sub & 1) != 0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const float send = h4 ? v[q] : v[q + 8];
+    const float keep = h4 ? v[q + 8] : v[q];
+    v[q] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float send = h2 ? v[q] : v[q + 4];
+    const float keep = h2 ? v[q + 4] : v[q];
+    v[q] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+  }
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const float send = h1 ? v[q] : v[q + 2];
+    const float keep = h1 ? v[q + 2] : v[q];
+    v[q] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
+  }
+}
+
 // Surrogate potential U_sur of the walker (cell context from cc), and with
 // kForces its forces into arr.F and the sums F.F, F.dir.  Group-uniform.
-// Requires a 512-thread CTA group.
+// Requires a 512-thread CTA: thread t serves atom t / 8 with the neighbours
+// j = t mod 8, t mod 8 + 8, ..., and warp w the row tile w / 4 of the
+// products; the four warps of a row tile meet at their own named barrier.
+// Every sum runs in a fixed order (deterministic results).
 template <bool kForces, bool kDiag, class G>
 __device__ __forceinline__ void sur_eval(Walker<G>& w, const MicRegs& cc, double& U, double& sff,
                                          double& sfd) {
   const WalkArrays& arr = w.arr;
-  WalkShared& s = w.s;
   const JrSurrogate& S = *w.sur;
   const int n = w.n;
-  const int np = n * (n - 1) / 2;
-  const int tid = w.g.rank(), gs = w.g.size();
-  const int lane = tid & 31, warp = tid >> 5, nwarps = gs >> 5;
-  uint64_t* nbm = arr.nbm + (w.swpar & 1) * kSWMaxAtoms;
-  uint64_t* nbm_next = arr.nbm + ((w.swpar + 1) & 1) * kSWMaxAtoms;
-  w.swpar ^= 1;
-  const float rc2 = kSurRc * kSurRc;
-  const int per_warp = ((np + gs - 1) / gs) * 32;
-  // ---- 1. scan: candidates within the cutoff, their (dr, r^2), masks ----
+  const int tid = w.g.rank();
+  const int lane = tid & 31, warp = tid >> 5;
+  const int grp = warp >> 2;
+  const int ai = tid >> 3, sub = tid & 7;
+  constexpr float kRc2 = kSurRc * kSurRc;
+  constexpr float kInvDmu = 1.0f / kSurDmu;
+  const float4 xi = arr.xs[ai < n ? ai : 0];
+  // ---- 1. descriptors of atom ai over its neighbour share, then the sum
+  // over the atom's 8 threads ----
   {
-    uint16_t* seg = arr.cand + warp * per_warp;
-    int cw = 0;
-    for (int p0 = warp * 32; p0 < np; p0 += gs) {
-      const int p = p0 + lane;
-      bool in = false;
-      float dx = 0.0f, dy = 0.0f, dz = 0.0f, r2 = 0.0f;
-      uint32_t ab = 0;
-      if (p < np) {
-        ab = arr.pij[p];
-        const float4 xa = arr.xs[ab & 255], xb = arr.xs[ab >> 8];
-        dx = __fsub_rn(xb.x, xa.x);
-        dy = __fsub_rn(xb.y, xa.y);
-        dz = __fsub_rn(xb.z, xa.z);
+    float ds[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) ds[k] = 0.0f;
+    if (ai < n) {
+      for (int j = sub; j < n; j += 8) {
+        const float4 xj = arr.xs[j];
+        float dx = __fsub_rn(xj.x, xi.x), dy = __fsub_rn(xj.y, xi.y), dz = __fsub_rn(xj.z, xi.z);
         mic_r<kDiag>(cc, dx, dy, dz);
-        r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-        in = r2 < rc2 && r2 > 0.0f;
+        const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+        if (j != ai && r2 < kRc2 && r2 > 0.0f) {
+          const float r = sqrtf(r2);
+          float fc, dfc, g[16];
+          sur_cutoff(r, fc, dfc);
+          sur_gauss16((r - kSurMu0) * kInvDmu, g);
+          fc *= kSurGScale;
+#pragma unroll
+          for (int k = 0; k < 16; ++k) ds[k] = fmaf(g[k], fc, ds[k]);
+        }
       }
-      const unsigned bal = __ballot_sync(0xffffffffu, in);
-      if (in) {
-        seg[cw + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)p;
-        arr.swr0[p] = make_float4(dx, dy, dz, r2);
-        unsigned* m32 = reinterpret_cast<unsigned*>(nbm);
-        const int a = ab & 255, b = ab >> 8;
-        atomicOr(m32 + 2 * a + (b >> 5), 1u << (b & 31));
-        atomicOr(m32 + 2 * b + (a >> 5), 1u << (a & 31));
-      }
-      cw += __popc(bal);
     }
-    if (lane == 0) s.sw_cand[warp] = cw;
+    sum16_over8(ds, sub);
+    const int k0 = 2 * sub;
+    const float x0 = ai < n ? fmaf(ds[0], S.in_scale[k0], S.in_shift[k0]) : 0.0f;
+    const float x1 = ai < n ? fmaf(ds[1], S.in_scale[k0 + 1], S.in_shift[k0 + 1]) : 0.0f;
+    *reinterpret_cast<uint32_t*>(arr.sx + ai * kSurLdX + k0) = sur_pack_bf16(x0, x1);
   }
-  w.g.sync();
-  int incl = lane < nwarps ? s.sw_cand[lane] : 0;
-  for (int off = 1; off < 32; off <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, incl, off);
-    if (lane >= off) incl += y;
-  }
-  const int M = __shfl_sync(0xffffffffu, incl, nwarps - 1);
-  // ---- 2. per pair: r, the cutoff and its derivative; the dense list ----
-  uint16_t* dense = arr.cand + kSWCandDense;
-  for (int base = tid - lane; base < M; base += gs) {
-    const int q = base + lane;
-    const int p = sw_cand_pair(arr.cand, per_warp, incl, nwarps, q < M ? q : M - 1);
-    if (q < M) {
-      dense[q] = (uint16_t)p;
-      const float4 d = arr.swr0[p];
-      const float r = sqrtf(d.w);
-      float fc, dfc;
-      sur_cutoff(r, fc, dfc);
-      arr.swr0[p] = make_float4(d.x, d.y, d.z, r);
-      arr.swr1[p] = make_float4(fc, dfc, 0.0f, 0.0f);
-    }
-  }
-  w.g.sync();
-  for (int q = tid; q < n; q += gs) nbm_next[q] = 0ull;  // the next evaluation's masks
-  // ---- 3. descriptors: thread (atom i, basis pair kk), neighbours ascending ----
-  for (int t = tid; t < 64 * 8; t += gs) {
-    const int i = t >> 3, k0 = 2 * (t & 7);
-    float d0 = 0.0f, d1 = 0.0f;
-    if (i < n) {
-      for (uint64_t m = nbm[i]; m; m &= m - 1) {
-        const int j = __ffsll((long long)m) - 1;
-        const int p = i < j ? sw_pidx(i, j, n) : sw_pidx(j, i, n);
-        const float r = arr.swr0[p].w;
-        const float4 c = arr.swr1[p];
-        float phi, dphi;
-        sur_basis(r, c.x, c.y, k0, phi, dphi);
-        d0 += phi;
-        sur_basis(r, c.x, c.y, k0 + 1, phi, dphi);
-        d1 += phi;
-      }
-      d0 = d0 * S.in_scale[k0] + S.in_shift[k0];
-      d1 = d1 * S.in_scale[k0 + 1] + S.in_shift[k0 + 1];
-    }
-    *reinterpret_cast<uint32_t*>(arr.sx + i * kSurLdX + k0) =
-        i < n ? sur_pack_bf16(d0, d1) : 0u;
-  }
-  w.g.sync();
-  // ---- 4. hidden layers: warp w owns row tile mt = w / 4 and the column
-  // tiles nt0 = 2 (w % 4), nt0 + 1 ----
-  const int mt = warp >> 2, nt0 = 2 * (warp & 3);
-  const int g = lane >> 2, cq = 2 * (lane & 3);
-  const int row_a = 16 * mt + g, row_b = row_a + 8;
+  rows_sync(grp);
+  // ---- 2. first layer: warp w owns row tile grp, column tiles nt0, nt0+1 ----
+  const int nt0 = 2 * (warp & 3);
+  const int g8 = lane >> 2, cq = 2 * (lane & 3);
+  const int row_a = 16 * grp + g8, row_b = row_a + 8;
   float ds1[8], g2[8];
   {
     uint32_t af[4], bf[2];
-    frag_a(arr.sx, kSurLdX, 16 * mt, 0, lane, af);
+    frag_a(arr.sx, kSurLdX, 16 * grp, 0, lane, af);
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
       float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
@@ -195,23 +198,27 @@ __device__ __forceinline__ void sur_eval(Walker<G>& w, const MicRegs& cc, double
       const int col = 8 * (nt0 + u) + cq;
       const float z00 = c[0] + arr.sbias[col], z01 = c[1] + arr.sbias[col + 1];
       const float z10 = c[2] + arr.sbias[col], z11 = c[3] + arr.sbias[col + 1];
-      ds1[4 * u] = sur_dsilu(z00);
-      ds1[4 * u + 1] = sur_dsilu(z01);
-      ds1[4 * u + 2] = sur_dsilu(z10);
-      ds1[4 * u + 3] = sur_dsilu(z11);
+      if (kForces) {
+        ds1[4 * u] = sur_dsilu(z00);
+        ds1[4 * u + 1] = sur_dsilu(z01);
+        ds1[4 * u + 2] = sur_dsilu(z10);
+        ds1[4 * u + 3] = sur_dsilu(z11);
+      }
       *reinterpret_cast<uint32_t*>(arr.sh1 + row_a * kSurLdH + col) =
           sur_pack_bf16(sur_silu(z00), sur_silu(z01));
       *reinterpret_cast<uint32_t*>(arr.sh1 + row_b * kSurLdH + col) =
           sur_pack_bf16(sur_silu(z10), sur_silu(z11));
     }
   }
-  w.g.sync();
+  rows_sync(grp);
+  // ---- 3. second layer and the per-row energies of this warp's columns ----
+  double e_part = 0.0;
   {
     float c[2][4] = {{0.0f, 0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f, 0.0f}};
 #pragma unroll
     for (int ks = 0; ks < 4; ++ks) {
       uint32_t af[4], bf[2];
-      frag_a(arr.sh1, kSurLdH, 16 * mt, 16 * ks, lane, af);
+      frag_a(arr.sh1, kSurLdH, 16 * grp, 16 * ks, lane, af);
 #pragma unroll
       for (int u = 0; u < 2; ++u) {
         frag_b(arr.sw2t, kSurLdH, 8 * (nt0 + u), 16 * ks, lane, bf);
@@ -227,29 +234,23 @@ __device__ __forceinline__ void sur_eval(Walker<G>& w, const MicRegs& cc, double
       const float z00 = c[u][0] + b0, z01 = c[u][1] + b1, z10 = c[u][2] + b0, z11 = c[u][3] + b1;
       ea += sur_silu(z00) * w0 + sur_silu(z01) * w1;
       eb += sur_silu(z10) * w0 + sur_silu(z11) * w1;
-      g2[4 * u] = S.out_scale * w0 * sur_dsilu(z00);
-      g2[4 * u + 1] = S.out_scale * w1 * sur_dsilu(z01);
-      g2[4 * u + 2] = S.out_scale * w0 * sur_dsilu(z10);
-      g2[4 * u + 3] = S.out_scale * w1 * sur_dsilu(z11);
+      if (kForces) {
+        g2[4 * u] = S.out_scale * w0 * sur_dsilu(z00);
+        g2[4 * u + 1] = S.out_scale * w1 * sur_dsilu(z01);
+        g2[4 * u + 2] = S.out_scale * w0 * sur_dsilu(z10);
+        g2[4 * u + 3] = S.out_scale * w1 * sur_dsilu(z11);
+      }
     }
-    // the four lanes of a row hold its 16 columns of this warp
     ea += __shfl_xor_sync(0xffffffffu, ea, 1);
     ea += __shfl_xor_sync(0xffffffffu, ea, 2);
     eb += __shfl_xor_sync(0xffffffffu, eb, 1);
     eb += __shfl_xor_sync(0xffffffffu, eb, 2);
-    if ((lane & 3) == 0) {
-      arr.separt[(warp & 3) * 64 + row_a] = ea;
-      arr.separt[(warp & 3) * 64 + row_b] = eb;
-    }
-  }
-  w.g.sync();
-  // ---- 5. energy: U = sum_i (e_i out_scale + out_shift), rows i < n ----
-  double e_part = 0.0;
-  if (tid < n) {
-    const float e = ((arr.separt[tid] + arr.separt[64 + tid]) +
-                     (arr.separt[128 + tid] + arr.separt[192 + tid])) +
-                    S.params[kSurOffB3];
-    e_part = (double)e * (double)S.out_scale + (double)S.out_shift;
+    // U = out_scale sum_{rows < n} (h2 . w3) + n (b3 out_scale + out_shift)
+    if ((lane & 3) == 0) e_part = (double)(row_a < n ? ea : 0.0f) + (double)(row_b < n ? eb : 0.0f);
+    e_part *= (double)S.out_scale;
+    if (tid == 0)
+      e_part += (double)n * ((double)S.params[kSurOffB3] * (double)S.out_scale +
+                             (double)S.out_shift);
   }
   if constexpr (!kForces) {
     double z0 = 0.0, z1 = 0.0;
@@ -258,8 +259,8 @@ __device__ __forceinline__ void sur_eval(Walker<G>& w, const MicRegs& cc, double
     sff = 0.0;
     sfd = 0.0;
   } else {
-    // ---- 6. backward: G2 -> G1 = (G2 W2^T) silu'(z1) -> dU/dx = G1 W1^T ----
-  #pragma unroll
+    // ---- 4. backward: G2 -> G1 = (G2 W2^T) silu'(z1) -> dU/dx = G1 W1^T ----
+#pragma unroll
     for (int u = 0; u < 2; ++u) {
       const int col = 8 * (nt0 + u) + cq;
       *reinterpret_cast<uint32_t*>(arr.sg2 + row_a * kSurLdH + col) =
@@ -267,20 +268,20 @@ __device__ __forceinline__ void sur_eval(Walker<G>& w, const MicRegs& cc, double
       *reinterpret_cast<uint32_t*>(arr.sg2 + row_b * kSurLdH + col) =
           sur_pack_bf16(g2[4 * u + 2], g2[4 * u + 3]);
     }
-    w.g.sync();
+    rows_sync(grp);
     {
       float c[2][4] = {{0.0f, 0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f, 0.0f}};
-  #pragma unroll
+#pragma unroll
       for (int ks = 0; ks < 4; ++ks) {
         uint32_t af[4], bf[2];
-        frag_a(arr.sg2, kSurLdH, 16 * mt, 16 * ks, lane, af);
-  #pragma unroll
+        frag_a(arr.sg2, kSurLdH, 16 * grp, 16 * ks, lane, af);
+#pragma unroll
         for (int u = 0; u < 2; ++u) {
           frag_b(arr.sw2k, kSurLdH, 8 * (nt0 + u), 16 * ks, lane, bf);
           mma_bf16(c[u], af, bf);
         }
       }
-  #pragma unroll
+#pragma unroll
       for (int u = 0; u < 2; ++u) {
         const int col = 8 * (nt0 + u) + cq;
         *reinterpret_cast<uint32_t*>(arr.sg1 + row_a * kSurLdH + col) =
@@ -289,60 +290,72 @@ __device__ __forceinline__ void sur_eval(Walker<G>& w, const MicRegs& cc, double
             sur_pack_bf16(c[u][2] * ds1[4 * u + 2], c[u][3] * ds1[4 * u + 3]);
       }
     }
-    w.g.sync();
-    if (warp < 8) {  // dU/dx [64][16]: row tile warp / 2, column tile warp % 2
-      const int m2 = warp >> 1, n2 = warp & 1;
+    rows_sync(grp);
+    if ((warp & 3) < 2) {  // dU/dD of the row tile: column tile warp & 1
+      const int n2 = warp & 1;
       float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-  #pragma unroll
+#pragma unroll
       for (int ks = 0; ks < 4; ++ks) {
         uint32_t af[4], bf[2];
-        frag_a(arr.sg1, kSurLdH, 16 * m2, 16 * ks, lane, af);
+        frag_a(arr.sg1, kSurLdH, 16 * grp, 16 * ks, lane, af);
         frag_b(arr.sw1k, kSurLdH, 8 * n2, 16 * ks, lane, bf);
         mma_bf16(c, af, bf);
       }
-      const int col = 8 * n2 + cq, ra = 16 * m2 + g;
-      arr.sdx[ra * 16 + col] = c[0] * S.in_scale[col];          // dU/dD
-      arr.sdx[ra * 16 + col + 1] = c[1] * S.in_scale[col + 1];
-      arr.sdx[(ra + 8) * 16 + col] = c[2] * S.in_scale[col];
-      arr.sdx[(ra + 8) * 16 + col + 1] = c[3] * S.in_scale[col + 1];
+      const int col = 8 * n2 + cq;
+      arr.sdx[row_a * kSurLdG + col] = c[0] * S.in_scale[col];
+      arr.sdx[row_a * kSurLdG + col + 1] = c[1] * S.in_scale[col + 1];
+      arr.sdx[row_b * kSurLdG + col] = c[2] * S.in_scale[col];
+      arr.sdx[row_b * kSurLdG + col + 1] = c[3] * S.in_scale[col + 1];
     }
     w.g.sync();
-    // ---- 7. pair forces: Q_ab = [sum_k (gD_ak + gD_bk) dphi_k(r) / r] dr_ab ----
-    for (int q = tid; q < M; q += gs) {
-      const int p = dense[q];
-      const uint32_t ab = arr.pij[p];
-      const int a = ab & 255, b = ab >> 8;
-      const float4 d = arr.swr0[p];
-      const float4 cf = arr.swr1[p];
-      float sk = 0.0f;
-  #pragma unroll
-      for (int k = 0; k < kSurBasis; ++k) {
-        float phi, dphi;
-        sur_basis(d.w, cf.x, cf.y, k, phi, dphi);
-        sk += (arr.sdx[a * 16 + k] + arr.sdx[b * 16 + k]) * dphi;
+    // ---- 5. forces: F_i = sum_j c_ij (x_j - x_i), c_ij = sum_k (dU/dD_ik +
+    // dU/dD_jk) dphi_k(r_ij) / r_ij, atom ai over its neighbour share, then
+    // the sum over its 8 threads ----
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+    if (ai < n) {
+      float gi[16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) gi[k] = arr.sdx[ai * kSurLdG + k];
+      for (int j = sub; j < n; j += 8) {
+        const float4 xj = arr.xs[j];
+        float dx = __fsub_rn(xj.x, xi.x), dy = __fsub_rn(xj.y, xi.y), dz = __fsub_rn(xj.z, xi.z);
+        mic_r<kDiag>(cc, dx, dy, dz);
+        const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+        if (j != ai && r2 < kRc2 && r2 > 0.0f) {
+          const float r = sqrtf(r2);
+          const float t = (r - kSurMu0) * kInvDmu;
+          float fc, dfc, g[16];
+          sur_cutoff(r, fc, dfc);
+          sur_gauss16(t, g);
+          fc *= kSurGScale;
+          dfc *= kSurGScale;
+          float sk = 0.0f;
+#pragma unroll
+          for (int k = 0; k < 16; ++k) {
+            const float dphi = g[k] * fmaf(-fc * kInvDmu, t - (float)k, dfc);
+            sk = fmaf(gi[k] + arr.sdx[j * kSurLdG + k], dphi, sk);
+          }
+          const float coef = sk / r;
+          fx = fmaf(coef, dx, fx);
+          fy = fmaf(coef, dy, fy);
+          fz = fmaf(coef, dz, fz);
+        }
       }
-      const float coef = sk / d.w;
-      arr.swq[p] = make_float4(coef * d.x, coef * d.y, coef * d.z, 0.0f);
     }
-    w.g.sync();
-    // ---- 8. gather, one lane per atom, neighbours ascending ----
+#pragma unroll
+    for (int off = 1; off < 8; off <<= 1) {
+      fx += __shfl_xor_sync(0xffffffffu, fx, off);
+      fy += __shfl_xor_sync(0xffffffffu, fy, off);
+      fz += __shfl_xor_sync(0xffffffffu, fz, off);
+    }
     double ff_part = 0.0, fd_part = 0.0;
-    for (int i = tid; i < n; i += gs) {
-      float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-      for (uint64_t m = nbm[i]; m; m &= m - 1) {
-        const int j = __ffsll((long long)m) - 1;
-        const bool fwd = i < j;
-        const float4 q = arr.swq[fwd ? sw_pidx(i, j, n) : sw_pidx(j, i, n)];
-        fx += fwd ? q.x : -q.x;
-        fy += fwd ? q.y : -q.y;
-        fz += fwd ? q.z : -q.z;
-      }
-      arr.F[3 * i] = fx;
-      arr.F[3 * i + 1] = fy;
-      arr.F[3 * i + 2] = fz;
-      const double dx = fx, dy = fy, dz = fz;
-      ff_part += dx * dx + dy * dy + dz * dz;
-      fd_part += dx * arr.dir[3 * i] + dy * arr.dir[3 * i + 1] + dz * arr.dir[3 * i + 2];
+    if (sub == 0 && ai < n) {
+      arr.F[3 * ai] = fx;
+      arr.F[3 * ai + 1] = fy;
+      arr.F[3 * ai + 2] = fz;
+      const double dfx = fx, dfy = fy, dfz = fz;
+      ff_part = dfx * dfx + dfy * dfy + dfz * dfz;
+      fd_part = dfx * arr.dir[3 * ai] + dfy * arr.dir[3 * ai + 1] + dfz * arr.dir[3 * ai + 2];
     }
     w.g.sum3(e_part, ff_part, fd_part, 1, w.par);
     U = e_part;

@@ -37,10 +37,12 @@ constexpr int kSurOffB3 = kSurOffW3 + kSurHidden;
 constexpr int kSurParams = kSurOffB3 + 1;
 static_assert(kSurParams == JR_SUR_PARAMS, "flat parameter layout");
 
-__device__ __forceinline__ float sur_silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU and its derivative with the approximate exponential and division
+// (a few ulp; the network's products round to bfloat16 anyway).
+__device__ __forceinline__ float sur_silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 
 __device__ __forceinline__ float sur_dsilu(float z) {
-  const float s = 1.0f / (1.0f + __expf(-z));
+  const float s = __fdividef(1.0f, 1.0f + __expf(-z));
   return s * (1.0f + z * (1.0f - s));
 }
 

@@ -44,7 +44,7 @@ sur_energy_kernel(const JrModelParams mp, const __grid_constant__ JrSurrogate su
   }
   __syncthreads();
   double sff, sfd;
-  const double U = sur_ham<true>(w, 0, 0.0, sff, sfd);
+  const double U = forces ? sur_ham<true>(w, 0, 0.0, sff, sfd) : sur_ham<false>(w, 0, 0.0, sff, sfd);
   if (threadIdx.x == 0) energy_u[b] = U;
   if (forces)
     for (int q = threadIdx.x; q < 3 * n; q += blockDim.x)

@@ -229,17 +229,17 @@ struct WalkArrays {
   uint16_t* sg2;        // [64][kSurLdH]   gradient at the second layer
   uint16_t* sg1;        // [64][kSurLdH]   gradient at the first layer
   float* sbias;         // [3][64] b1, b2, w3
-  float* sdx;           // [64][16] gradient of the energy at the inputs
-  float* separt;        // [4][64] per-row energy partials of the column groups
+  float* sdx;           // [64][kSurLdG] gradient of the energy at the descriptors
 };
 
 // Padded row strides (bfloat16 elements) of the surrogate's operand tiles:
-// the warp-level fragment loads of 8 rows x 4 columns fall on distinct banks.
-constexpr int kSurLdX = 24, kSurLdH = 72;
+// the warp-level fragment loads of 8 rows x 4 columns fall on distinct banks;
+// kSurLdG (floats) spreads the dU/dD rows of neighbouring atoms over banks.
+constexpr int kSurLdX = 24, kSurLdH = 72, kSurLdG = 17;
 
 __host__ __device__ inline size_t sur_table_bytes() {
   return 2u * (64u * kSurLdX * 2u + 64u * kSurLdH * 5u + 16u * kSurLdH) + 4u * (3u * 64u) +
-         4u * (64u * 16u) + 4u * (4u * 64u);
+         4u * (64u * kSurLdG);
 }
 
 __host__ __device__ inline bool use_pair_matrix(int nmax, int nimg, int fam = kFamPair) {
@@ -309,7 +309,7 @@ __device__ inline WalkShared* carve_walker(char* p, int nmax, int nimg, const ui
   a.nbm = nullptr;
   a.cand = nullptr;
   a.sw1t = a.sw2t = a.sw2k = a.sw1k = a.sx = a.sh1 = a.sg2 = a.sg1 = nullptr;
-  a.sbias = a.sdx = a.separt = nullptr;
+  a.sbias = a.sdx = nullptr;
   if (use_pair_matrix(nmax, nimg, fam)) {
     a.pm = (float*)p;
     a.pij = pij;
@@ -335,8 +335,7 @@ __device__ inline WalkShared* carve_walker(char* p, int nmax, int nimg, const ui
     a.sg1 = (uint16_t*)q; q += 2 * 64 * kSurLdH;
     a.sw1k = (uint16_t*)q; q += 2 * 16 * kSurLdH;
     a.sbias = (float*)q; q += 4 * 3 * 64;
-    a.sdx = (float*)q; q += 4 * 64 * 16;
-    a.separt = (float*)q; q += 4 * 4 * 64;
+    a.sdx = (float*)q; q += 4 * 64 * kSurLdG;
     p += align16(sur_table_bytes());
   }
   a.nz = use_normal_buffer(nmax, normals) ? (float*)p : nullptr;

@@ -34,6 +34,14 @@ from .nested_sampling import (InfoBuffers, NSState, _stream, make_dims, ns_itera
 from .surrogate import Surrogate
 
 
+def torch_det_abs(cell):
+    """|det| of (..., 3, 3) cells in float64 (the triple product, elementwise)."""
+    import torch
+
+    c = cell.to(torch.float64)
+    return (c[..., 0, :] * torch.linalg.cross(c[..., 1, :], c[..., 2, :])).sum(-1).abs()
+
+
 class SampleRing:
     """Device ring of exactly evaluated configurations: positions
     ``(capacity, Nmax, 3)``, cells ``(capacity, 3, 3)`` and model energies
@@ -184,7 +192,7 @@ class DelayedAcceptanceNS:
                  n_mcmc_steps: int = 20, ring_capacity: int = 100_000, train_every: int = 50,
                  train_window: int = 100_000, train_steps: int = 16, batch: int = 256,
                  lr: float = 1e-3, warmup_iters: int = 0, bootstrap_steps: int = 200,
-                 seed: int = 0):
+                 margin: float = 0.5, seed: int = 0):
         import torch
 
         self.ns = ns_state
@@ -199,6 +207,7 @@ class DelayedAcceptanceNS:
         self.batch = int(batch)
         self.lr = float(lr)
         self.warmup_iters = int(warmup_iters)
+        self.margin = float(margin)
         self.bootstrap_steps = int(bootstrap_steps)
         self.gen = torch.Generator(device=device()).manual_seed(seed)
         self.since_train = 0
@@ -211,13 +220,21 @@ class DelayedAcceptanceNS:
         B, N, _ = positions.shape
         return _evaluate(model, None, positions, np.zeros(N, np.int32), cells, False).energy
 
-    def bootstrap(self) -> None:
+    def bootstrap(self, positions=None, cells=None) -> None:
+        """Fill the ring with the live population, the configurations
+        ``positions`` (B, N, 3) / ``cells`` (B, 3, 3) when given (e.g. the dead
+        walkers of earlier iterations) and the dead walkers of
+        ``warmup_iters`` plain iterations, all evaluated exactly; then set the
+        normalisation, train and calibrate."""
         import torch
 
         pop = self.ns.population
         P, K, N = pop.types.shape
         xs = [pop.positions.reshape(P * K, N, 3).clone()]
         cs = [pop.cell.reshape(P * K, 3, 3).clone()]
+        if positions is not None:
+            xs.append(torch.as_tensor(positions, device=device()).reshape(-1, N, 3))
+            cs.append(torch.as_tensor(cells, device=device()).reshape(-1, 3, 3))
         if self.warmup_iters > 0:
             info = ns_iterate(self.ns, self.step_fn, self.warmup_iters, self.T)
             xs.append(info.dead_positions.reshape(-1, N, 3))
@@ -229,21 +246,79 @@ class DelayedAcceptanceNS:
         self.ring.push(x, c, U)
         D = Surrogate.descriptors(x, c)
         self.sur.fit_normalisation(D, U, N)
-        self.train(self.bootstrap_steps)
+        self.train(self.bootstrap_steps, renormalise=True)
 
-    def train(self, steps: int) -> None:
+    def _live_u_max(self):
+        """The largest per-atom model energy of the live walkers (float)."""
         import torch
 
+        pop = self.ns.population
+        P, K, N = pop.types.shape
+        vol = torch_det_abs(pop.cell)
+        pr = pop.ensemble_params.get("pressure", 0.0)
+        pr = torch.as_tensor(pr, dtype=torch.float64, device=vol.device).reshape(-1, 1)
+        u = (pop.energy64 - pr * vol) / N
+        return float(u.max())
+
+    def training_set(self):
+        """Ring slots to train and calibrate on: the last ``train_window``
+        evaluated slots whose per-atom energy lies below the highest live
+        walker's plus ``margin`` eV (the configurations near and inside the
+        contour, where stage 1 decides)."""
         idx = self.ring.recent_valid(self.train_window)
+        if idx.numel() == 0:
+            return idx
+        N = self.ring.n_atoms_max
+        keep = self.ring.energy_u[idx] / N <= self._live_u_max() + self.margin
+        return idx[keep]
+
+    def calibrate(self, idx=None, n: int = 512) -> tuple[float, float]:
+        """Set the surrogate constraint from its error d = U_sur - U on
+        recent training configurations: ``contour_shift`` = median(d),
+        ``tau`` = 0.6 x 1.4826 MAD(d) (a logistic of that scale follows the
+        normal CDF of the error), at least 1e-3.  Either choice leaves the walk
+        exact; they set how well stage 1 screens.  Returns (shift, tau)."""
+        import torch
+
+        idx = self.training_set() if idx is None else idx
+        if idx.numel() == 0:
+            return self.sur.contour_shift, self.sur.tau
+        idx = idx[-n:]
+        Us, _ = surrogate_energy_forces(self.sur, self.ring.positions[idx],
+                                        self.ring.cell[idx], forces=False)
+        d = Us - self.ring.energy_u[idx]
+        med = d.median()
+        mad = (d - med).abs().median()
+        self.sur.contour_shift = float(med)
+        self.sur.tau = max(0.6 * 1.4826 * float(mad), 1e-3)
+        return self.sur.contour_shift, self.sur.tau
+
+    def train(self, steps: int, renormalise: bool = False) -> None:
+        """``steps`` Adam steps on minibatches of the training set (after
+        refitting the standardisation to it when ``renormalise``); then
+        recalibrate."""
+        import torch
+
+        idx = self.training_set()
         if idx.numel() == 0 or steps <= 0:
             return
+        N = self.ring.n_atoms_max
+        if renormalise:
+            sub = idx[-4096:]
+            D = Surrogate.descriptors(self.ring.positions[sub], self.ring.cell[sub])
+            self.sur.renormalise(D, self.ring.energy_u[sub], N)
         B = min(self.batch, int(idx.numel()))
-        ar = torch.arange(B, dtype=torch.int32, device=idx.device)
-        for _ in range(steps):
-            pick = idx[torch.randint(0, idx.numel(), (B,), generator=self.gen, device=idx.device)]
-            D = Surrogate.descriptors(self.ring.positions[pick], self.ring.cell[pick])
-            self.sur.train_step(D, self.ring.energy_u[pick].contiguous(), ar, self.lr)
+        # every minibatch of the round drawn at once: one descriptor launch,
+        # then one training launch per minibatch on its rows
+        pick = idx[torch.randint(0, idx.numel(), (steps * B,), generator=self.gen,
+                                 device=idx.device)]
+        D = Surrogate.descriptors(self.ring.positions[pick], self.ring.cell[pick])
+        Ub = self.ring.energy_u[pick].contiguous()
+        rows = torch.arange(steps * B, dtype=torch.int32, device=idx.device).view(steps, B)
+        for k in range(steps):
+            self.sur.train_step(D, Ub, rows[k], self.lr)
         self.since_train = 0
+        self.calibrate(idx)
 
     def run(self, n_iter: int, block: int = 10):
         """Walk ``n_iter`` iterations; returns the info buffers of the last

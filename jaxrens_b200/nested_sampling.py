@@ -64,6 +64,20 @@ class NSState:
     def set(self, **kw) -> NSState:
         return dataclasses.replace(self, **kw)
 
+    def clone(self) -> NSState:
+        """An independent copy: every device buffer copied."""
+        import torch
+
+        def c(v):
+            return v.clone() if isinstance(v, torch.Tensor) else v
+
+        pop = dataclasses.replace(self.population, **{
+            f.name: c(getattr(self.population, f.name))
+            for f in dataclasses.fields(self.population)})
+        return dataclasses.replace(self, population=pop, log_evidence=c(self.log_evidence),
+                                   iteration=c(self.iteration), emax=c(self.emax),
+                                   rng_key=c(self.rng_key), workspace=c(self.workspace))
+
     @property
     def n_runs(self) -> int:
         return int(self.log_evidence.shape[0])

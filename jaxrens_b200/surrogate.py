@@ -131,6 +131,34 @@ class Surrogate:
         self.out_shift = float(u.mean())
         self.out_scale = float(max(float(u.std()), 1e-3))
 
+    def renormalise(self, D, U, n_atoms: int) -> None:
+        """Refit the input and output standardisation to (D, U) while keeping
+        the function the network computes: W1 and b1 absorb the change of
+        the input affine map, w3 and b3 the change of the output one.  The
+        Adam moments restart."""
+        import torch
+
+        a, b = np.asarray(self.in_scale, np.float64), np.asarray(self.in_shift, np.float64)
+        s, t = float(self.out_scale), float(self.out_shift)
+        self.fit_normalisation(D, U, n_atoms)
+        a2, b2 = np.asarray(self.in_scale, np.float64), np.asarray(self.in_shift, np.float64)
+        s2, t2 = float(self.out_scale), float(self.out_shift)
+        p = self.params.double()
+        W1 = p[OFF_W1:OFF_B1].view(N_BASIS, HIDDEN)
+        r = torch.as_tensor(a / a2, dtype=torch.float64, device=p.device)
+        c = torch.as_tensor(b - b2 * (a / a2), dtype=torch.float64, device=p.device)
+        b1 = p[OFF_B1:OFF_W2] + c @ W1
+        W1 = W1 * r[:, None]
+        w3 = p[OFF_W3:OFF_B3] * (s / s2)
+        b3 = (p[OFF_B3] * s + t - t2) / s2
+        self.params[OFF_W1:OFF_B1] = W1.reshape(-1).float()
+        self.params[OFF_B1:OFF_W2] = b1.float()
+        self.params[OFF_W3:OFF_B3] = w3.float()
+        self.params[OFF_B3] = b3.float()
+        self.adam_m.zero_()
+        self.adam_v.zero_()
+        self.step = 0
+
     # ------------------------------------------------------- training ----
     def train_step(self, D, U, batch_idx, lr: float = 1e-3) -> None:
         """One Adam step on the configurations batch_idx (int32, device) of

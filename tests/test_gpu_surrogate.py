@@ -122,3 +122,21 @@ def test_training_lowers_the_loss_on_stillinger_weber_energies():
     last = sur.fit(D, Ut, epochs=60, batch=64, lr=3e-3)
     assert not sur.train_error()
     assert last < 0.2 * first, (first, last)
+
+
+def test_renormalise_keeps_the_function():
+    """Refitting the standardisation rewrites W1, b1, w3 and b3 so that the
+    float64 network computes the same energies as before."""
+    x, c = _configs(41, 6)
+    sur = _surrogate_with(8)
+    before = _ref_params(sur)
+    xs, cs = perturbed_diamond(3, 16)
+    D = sg.Surrogate.descriptors(xs, cs)
+    U = torch.as_tensor(np.linspace(-200.0, -150.0, 16), dtype=torch.float64)
+    sur.renormalise(D, U, 64)
+    after = _ref_params(sur)
+    assert not np.allclose(before["in_scale"], after["in_scale"])
+    for b in range(len(x)):
+        e0 = S.energy(x[b], c[b], before, bf=False)
+        e1 = S.energy(x[b], c[b], after, bf=False)
+        assert abs(e0 - e1) <= 1e-5 * max(abs(e0), 1.0), (e0, e1)
