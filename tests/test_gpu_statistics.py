@@ -9,6 +9,10 @@
   reflections): GPU and oracle ensembles give the same log Z after 6000
   iterations (prior mass about 1e-5), so the throughput is measured at
   matched log Z.
+* LJ-32 on the bench's pressure ladder with replica exchange every 10
+  iterations, 16 seeds per arm: per pressure, log Z and the seed-mean contour
+  energy at fixed log X along the run agree with the oracle in the
+  reference's float32 arithmetic.
 """
 
 import numpy as np
@@ -122,3 +126,52 @@ def test_lj32_npt_bench_shape_log_z_matches_reference_arithmetic():
     print("final contour GPU %.4f +- %.4f, oracle %.4f +- %.4f" %
           (eg.mean(), eg.std(ddof=1), er.mean(), er.std(ddof=1)))
     assert abs(eg.mean() - er.mean()) < 4 * se_e + 1e-3 * abs(er.mean()), (eg, er)
+
+
+def test_lj32_pressure_ladder_with_replica_exchange_matches_reference_arithmetic():
+    """The bench's pressure ladder (8 runs at pressures log-spaced over
+    0.01-1.0, replica exchange every 10 iterations) with 16 independent seeds
+    per arm: the GPU walk and the oracle in the reference's float32
+    arithmetic.  Compared per pressure: log Z, and the low-variance statistic
+    of the seed-mean contour energy at fixed log X (every 100 iterations
+    along the run), each within 4 standard errors.  128 walkers of 32 atoms,
+    n_mcmc_steps 20, 10 reflections, 1500 iterations (log X = -11.7)."""
+    S, P, K, N, T, R, n_iter, every = 16, 8, 128, 32, 20, 10, 1500, 10
+    pressures = np.logspace(-2, 0, P).astype(np.float32)
+    la = prior_mass.log_alpha(K, 1)
+    wo = float(prior_mass.iteration_offsets(K, 1)[1][0])
+    dead = {"gpu": np.zeros((S, P, n_iter)), "ref": np.zeros((S, P, n_iter))}
+    lz = {"gpu": np.zeros((S, P)), "ref": np.zeros((S, P))}
+    for s in range(S):
+        c = lj_case(P=P, K=K, N=N, seed=1000 + s, n_reflect=R, T=T, pressure=pressures)
+        ns = nsm.init_ns_parallel(c["init_fn"], c["positions"], c["types"], c["energies"],
+                                  c["cells"], c["run_keys"],
+                                  ensemble_params={"pressure": c["pressures"]})
+        re = nsm.InterREManager(every, 1, prng.fold_in(prng.key(1000 + s), 5))
+        rows = []
+        for _ in range(n_iter // every):
+            info = nsm.ns_iterate(ns, c["step"], every, T)
+            rows.append(info.dead_energy.cpu().numpy())
+            re.apply(ns, c["step"])
+        dead["gpu"][s] = np.concatenate(rows, axis=0).T
+        live = ns.population.energy64.cpu().numpy()
+        lz["gpu"][s] = [thermo.log_evidence(dead["gpu"][s, r], live[r], K) for r in range(P)]
+        c = lj_case(P=P, K=K, N=N, seed=2000 + s, n_reflect=R, T=T, pressure=pressures)
+        reps = oracle_replicas(c)
+        re = nsm.InterREManager(every, 1, prng.fold_in(prng.key(2000 + s), 5))
+        for it in range(n_iter):
+            infos = O.ns_step_batched(c["model"], c["moves"], reps, T, la, wo,
+                                      shared_move_key=True, mode=O.REF32, n_threads=8)
+            dead["ref"][s, :, it] = [i.dead_energy for i in infos]
+            if (it + 1) % every == 0:
+                O.re_step(reps, re.next_swap_key(), 1, mode=O.REF32)
+        lz["ref"][s] = [thermo.log_evidence(dead["ref"][s, r], reps[r].energy, K)
+                        for r in range(P)]
+    for r in range(P):
+        a, b = lz["gpu"][:, r], lz["ref"][:, r]
+        se = np.sqrt(a.var(ddof=1) / S + b.var(ddof=1) / S)
+        assert abs(a.mean() - b.mean()) < 4 * se + 0.05, (r, a, b)
+        for it in range(every * 10 - 1, n_iter, 100):
+            a, b = dead["gpu"][:, r, it], dead["ref"][:, r, it]
+            se = np.sqrt(a.var(ddof=1) / S + b.var(ddof=1) / S)
+            assert abs(a.mean() - b.mean()) < 4 * se + 1e-6 * abs(b.mean()), (r, it, a, b)
