@@ -659,7 +659,8 @@ def _da_arm(name, ns, step, n_steps, walk, torch):
             "acceptance_per_move": (acc / prop).tolist(),
             "exact_evaluations_per_walker_step": float(nev.sum()) / ws,
             "exact_evaluations_per_move_step": (nev / prop).tolist(),
-            "surrogate_evaluations_per_walker_step": float(nsur.sum()) / ws}
+            "surrogate_evaluations_per_walker_step": float(nsur.sum()) / ws,
+            "mean_contour_after": float(ns.emax.double().mean())}
 
 
 def run_da(args):
