@@ -473,7 +473,7 @@ def end_to_end(args, ns, step, re, cfg, torch, nsm):
     # consecutive states (one step apart) in pinned host memory, as many as
     # the timed steps up to 32 (128 MB), so the end-to-end mean covers as many
     # trajectories as the device-resident one
-    n = max(3, args.steps // 2)
+    n = max(30, args.steps // 2)
     n_snap = min(n, 32)
     for f, v in zip(fields, [getattr(bufs[0][1].population, k) for k in names_p] +
                     [getattr(bufs[0][1], k) for k in names_s]):
