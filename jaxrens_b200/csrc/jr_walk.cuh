@@ -110,6 +110,33 @@ struct CtaG {
     c = __shfl_sync(0xffffffffu, c, 0);
     par ^= 1;
   }
+  // sum3 of one value: the same tree for `a`, a third of the shuffles
+  __device__ __forceinline__ void sum1(double& a, int stride, int& par) const {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int off = 16; off >= stride; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+    double (*buf)[3] = red[par];
+    if (lane == 0) buf[warp][0] = a;
+    __syncthreads();
+    // every thread sums the warp partials itself, in the pairwise order of
+    // sum3's butterfly (zeros past nw; x + 0 leaves x unchanged): no shuffle
+    // chain and no broadcast after the barrier
+    a = nw <= 8 ? tree_sum<8>(buf, nw) : tree_sum<16>(buf, nw);
+    par ^= 1;
+  }
+  // the pairwise sum of buf[0..nw)[0] padded with zeros to W entries (the
+  // launch bound of 512 threads keeps nw <= 16)
+  template <int W>
+  __device__ __forceinline__ static double tree_sum(const double (*buf)[3], int nw) {
+    double v[W];
+#pragma unroll
+    for (int q = 0; q < W; ++q) v[q] = q < nw ? buf[q][0] : 0.0;
+#pragma unroll
+    for (int st = 1; st < W; st <<= 1)
+#pragma unroll
+      for (int q = 0; q + st < W; q += 2 * st) v[q] += v[q + st];
+    return v[0];
+  }
 };
 
 // One warp walking one walker: register shuffles only, no block barriers.
@@ -133,6 +160,11 @@ struct WarpG {
       b = __shfl_sync(0xffffffffu, b, 0);
       c = __shfl_sync(0xffffffffu, c, 0);
     }
+    (void)par;
+  }
+  __device__ __forceinline__ void sum1(double& a, int stride, int& par) const {
+    for (int off = 16; off >= stride; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+    if (stride > 1) a = __shfl_sync(0xffffffffu, a, 0);
     (void)par;
   }
 };
@@ -744,8 +776,7 @@ __device__ __forceinline__ void pairs_matrix(const JrParams& P, Walker<G>& w, co
   }
   if (tid == 0) w.tc[kForces ? 0 : 2] += np;
   if (!kForces) {
-    double z0 = 0.0, z1 = 0.0;
-    w.g.sum3(ep, z0, z1, 1, w.par);
+    w.g.sum1(ep, 1, w.par);
     U = ep;
     sff = 0.0;
     sfd = 0.0;
@@ -901,7 +932,8 @@ __device__ __forceinline__ void pairs_ordered(const JrParams& P, Walker<G>& w, c
       }
     }
   }
-  w.g.sum3(e_part, ff_part, fd_part, 1, w.par);
+  if (kForces) w.g.sum3(e_part, ff_part, fd_part, 1, w.par);
+  else w.g.sum1(e_part, 1, w.par);
   U = 0.5 * e_part;
   sff = ff_part;
   sfd = fd_part;
@@ -991,8 +1023,7 @@ __device__ __forceinline__ double ham_eval(const JrParams& P, Walker<G>& w, int 
 
 template <class G>
 __device__ __forceinline__ double group_sum1(Walker<G>& w, double v) {
-  double b = 0.0, c = 0.0;
-  w.g.sum3(v, b, c, 1, w.par);
+  w.g.sum1(v, 1, w.par);
   return v;
 }
 
