@@ -594,8 +594,15 @@ __device__ __forceinline__ void mic_r(const MicRegs& m, float& dx, float& dy, fl
 // 1/x for the pair loop: a bit-pattern seed refined by three Newton-Raphson
 // steps y <- y + y*(1 - x*y), all in fused multiply-adds, so the result is the
 // same on any IEEE machine with an FMA (the CPU check reproduces it bit for
-// bit).  Max error 0.501 ulp over normal inputs; inputs outside [2^-120, 2^120]
-// (zero, denormals, inf, NaN) take the correctly rounded reciprocal.
+// bit).  The seed y0 = as_float(C - as_int(x)) is the piecewise-linear
+// reciprocal of the float bit pattern (the exponent negated, the mantissa
+// reflected); C sets its offset.  Scanning every C over the mantissas of one
+// binade, the largest relative error max|x*y0 - 1| is smallest at C =
+// 0x7EF311C2 (5.0510%), and C = 0x7EF311C3, used here, is within 2e-8 of it.
+// Each Newton step squares the relative error: 5.05% -> 2.6e-3 -> 6.5e-6 ->
+// 4e-11, below half an ulp before the last rounding.  Max error 0.501 ulp
+// over normal inputs; inputs outside [2^-120, 2^120] (zero, denormals, inf,
+// NaN) take the correctly rounded reciprocal.
 __device__ __noinline__ inline float rcp_rare(float x) { return __frcp_rn(x); }
 
 __device__ __forceinline__ float rcp_nr(float x) {

@@ -263,7 +263,11 @@ static int center_image(const JroModel* m) {
 }
 
 /* Kernel reciprocal: bit-pattern seed + three FMA Newton-Raphson steps
- * (max 0.501 ulp); outside [2^-120, 2^120] the correctly rounded 1/x. */
+ * (max 0.501 ulp); outside [2^-120, 2^120] the correctly rounded 1/x.  The
+ * seed as_float(C - as_int(x)) is the piecewise-linear reciprocal of the bit
+ * pattern; C = 0x7EF311C3 is within 2e-8 of the offset that minimises its
+ * largest relative error over a binade (5.05%, found by scanning C), and each
+ * Newton step squares that error. */
 static inline float rcp_nr(float x) {
   if (!(x >= 0x1p-120f && x <= 0x1p120f)) return 1.0f / x;
   uint32_t u;

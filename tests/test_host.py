@@ -335,3 +335,22 @@ def test_bernoulli_species_draws():
     b = prng.bernoulli(k, 4096, 0.5)
     np.testing.assert_array_equal(b, O.uniform(k, 4096) < np.float32(0.5))
     assert abs(b.mean() - 0.5) < 0.03
+
+
+def test_reciprocal_seed_is_near_minimax():
+    """The pair loop's reciprocal seed as_float(C - as_int(x)), C =
+    0x7EF311C3: over the mantissas of one binade its largest relative error
+    is 5.05%, within 1e-7 of the best offset a scan of C finds, and three
+    Newton steps bring it below 1e-10 before rounding."""
+    m = np.arange(0, 1 << 23, 13, dtype=np.uint32)
+    xb = (m | 0x3F800000).astype(np.int64)
+    x = (m | 0x3F800000).view(np.float32).astype(np.float64)
+
+    def err(c):
+        y = (np.int64(c) - xb).astype(np.uint32).view(np.float32).astype(np.float64)
+        return np.abs(y * x - 1.0).max()
+
+    e = err(0x7EF311C3)
+    best = min(err(c) for c in range(0x7EF311C3 - 256, 0x7EF311C3 + 256, 4))
+    assert 0.0504 < e < 0.0506 and e - best < 1e-7
+    assert e ** 8 < 1e-10
