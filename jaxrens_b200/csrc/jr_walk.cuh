@@ -95,19 +95,18 @@ struct CtaG {
       buf[warp][2] = c;
     }
     __syncthreads();
-    // lane q < nw takes warp q's partials (zero above); a butterfly over the
-    // lowest next_pow2(nw) lanes puts the totals in lane 0, which broadcasts
-    a = lane < nw ? buf[lane][0] : 0.0;
-    b = lane < nw ? buf[lane][1] : 0.0;
-    c = lane < nw ? buf[lane][2] : 0.0;
-    for (int off = 1; off < nw; off <<= 1) {
-      a += __shfl_xor_sync(0xffffffffu, a, off);
-      b += __shfl_xor_sync(0xffffffffu, b, off);
-      c += __shfl_xor_sync(0xffffffffu, c, off);
+    // every thread sums the warp partials itself: the pairwise tree over the
+    // lowest next_pow2(nw) warps (zeros above), no shuffle chain after the
+    // barrier
+    if (nw <= 8) {
+      a = tree_sum<8>(buf, nw, 0);
+      b = tree_sum<8>(buf, nw, 1);
+      c = tree_sum<8>(buf, nw, 2);
+    } else {
+      a = tree_sum<16>(buf, nw, 0);
+      b = tree_sum<16>(buf, nw, 1);
+      c = tree_sum<16>(buf, nw, 2);
     }
-    a = __shfl_sync(0xffffffffu, a, 0);
-    b = __shfl_sync(0xffffffffu, b, 0);
-    c = __shfl_sync(0xffffffffu, c, 0);
     par ^= 1;
   }
   // sum3 of one value: the same tree for `a`, a third of the shuffles
@@ -121,16 +120,17 @@ struct CtaG {
     // every thread sums the warp partials itself, in the pairwise order of
     // sum3's butterfly (zeros past nw; x + 0 leaves x unchanged): no shuffle
     // chain and no broadcast after the barrier
-    a = nw <= 8 ? tree_sum<8>(buf, nw) : tree_sum<16>(buf, nw);
+    a = nw <= 8 ? tree_sum<8>(buf, nw, 0) : tree_sum<16>(buf, nw, 0);
     par ^= 1;
   }
-  // the pairwise sum of buf[0..nw)[0] padded with zeros to W entries (the
-  // launch bound of 512 threads keeps nw <= 16)
+  // the pairwise sum of buf[0..nw)[k] padded with zeros to W entries (the
+  // launch bound of 512 threads keeps nw <= 16); the order of the butterfly
+  // over next_pow2(nw) lanes, since x + 0 leaves x unchanged
   template <int W>
-  __device__ __forceinline__ static double tree_sum(const double (*buf)[3], int nw) {
+  __device__ __forceinline__ static double tree_sum(const double (*buf)[3], int nw, int k) {
     double v[W];
 #pragma unroll
-    for (int q = 0; q < W; ++q) v[q] = q < nw ? buf[q][0] : 0.0;
+    for (int q = 0; q < W; ++q) v[q] = q < nw ? buf[q][k] : 0.0;
 #pragma unroll
     for (int st = 1; st < W; st <<= 1)
 #pragma unroll
