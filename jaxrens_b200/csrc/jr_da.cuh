@@ -253,8 +253,7 @@ __device__ __forceinline__ void sur_eval(Walker<G>& w, const MicRegs& cc, double
                              (double)S.out_shift);
   }
   if constexpr (!kForces) {
-    double z0 = 0.0, z1 = 0.0;
-    w.g.sum3(e_part, z0, z1, 1, w.par);
+    w.g.sum1(e_part, 1, w.par);
     U = e_part;
     sff = 0.0;
     sfd = 0.0;

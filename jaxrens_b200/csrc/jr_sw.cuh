@@ -311,8 +311,7 @@ __device__ __forceinline__ void sw_eval(const JrParams& P, Walker<G>& w, const M
   w.tc[kForces ? 1 : 3] += ntrip;
   ep += e3;
   if (!kForces) {
-    double z0 = 0.0, z1 = 0.0;
-    w.g.sum3(ep, z0, z1, 1, w.par);
+    w.g.sum1(ep, 1, w.par);
     U = ep;
     sff = 0.0;
     sfd = 0.0;
