@@ -47,6 +47,7 @@ struct NsShared {
   int cc[JR_MAX_CULL];     // n_cull > 1: their clone sources
   double ce[JR_MAX_CULL];  // n_cull > 1: culled energies
   double res_E[kMaxWarps];  // final energy of each chain this CTA walked
+  double vE[kMaxWalk];      // validation: every slot's final energy, gathered once
   unsigned long long u64[2][kMaxWarps];
   int flag[2][kMaxWarps];
 };
@@ -343,9 +344,14 @@ __device__ inline void predict_fast(NsShared& ns, const double* E, int K, int Dr
   // the lane that loses a walker to a cull rescans its entries
   unsigned long long lbest = 0;
   int lnan = 0;
+  // and how many of the lane's entries equal its largest value (== on the
+  // values: -0.0 ties with +0.0), with 1 + the largest such index
+  int lties = 0, lidx = 0;
   auto lane_scan = [&]() {
     lbest = 0;
     lnan = 0;
+    lties = 0;
+    lidx = 0;
     for (int j = 0; j < nslot; ++j) {
       const int k = lane + 32 * j;
       if (k >= K || ((taken >> j) & 1u)) continue;
@@ -354,7 +360,15 @@ __device__ inline void predict_fast(NsShared& ns, const double* E, int K, int Dr
         lnan = 1;
       } else {
         const unsigned long long o = ord_double(x);
-        lbest = o > lbest ? o : lbest;
+        if (o > lbest) {
+          const bool eq = lbest != 0 && x == unord_double(lbest);
+          lbest = o;
+          lties = eq ? lties + 1 : 1;
+          lidx = k + 1;
+        } else if (x == unord_double(lbest)) {
+          ++lties;
+          lidx = k + 1;
+        }
       }
     }
   };
@@ -377,12 +391,8 @@ __device__ inline void predict_fast(NsShared& ns, const double* E, int K, int Dr
       int nties = 0, idx1 = 0;
       // (== on the values: -0.0 ties with +0.0, as in the reference's E == max)
       if (lbest != 0 && unord_double(lbest) == emax) {
-        for (int j = 0; j < nslot; ++j) {
-          const int k = lane + 32 * j;
-          if (k >= K || ((taken >> j) & 1u) || E[k] != emax) continue;
-          ++nties;
-          idx1 = k + 1;
-        }
+        nties = lties;
+        idx1 = lidx;
       }
       int tot = nties, idx = idx1;
       for (int off = 16; off > 0; off >>= 1) {
@@ -683,15 +693,16 @@ ns_iterate_kernel(const JrDims D, const JrParams Pg, const JrStateBuffers st,
     // ---- validation: longest prefix whose predicted culls hold ----
     int nval = 1;
     if (Dmax > 1) {
+      // every slot's final energy, one remote load per thread, then the
+      // prefix test on the local copy
+      for (int sl = threadIdx.x; sl < Dr * W; sl += blockDim.x)
+        ns.vE[sl] = *cluster.map_shared_rank(&ns.res_E[sl % cpc], sl / cpc);
+      __syncthreads();
       nval = 0;
       for (int d = 0; d < Dr; ++d) {
         bool ok = ns.spec[d] != 0;
-        for (int d2 = 0; d2 < d && ok; ++d2)
-          for (int w2 = 0; w2 < W && ok; ++w2) {
-            const int sl = d2 * W + w2;
-            const double* r = cluster.map_shared_rank(&ns.res_E[sl % cpc], sl / cpc);
-            if (!(*r < ns.e[d])) ok = false;
-          }
+        for (int sl = 0; sl < d * W && ok; ++sl)
+          if (!(ns.vE[sl] < ns.e[d])) ok = false;
         if (!ok) break;
         ++nval;
       }
