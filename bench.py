@@ -693,7 +693,8 @@ def run_da(args):
     ns_exact, ns_untr = ns.clone(), ns.clone()
     drv = da.DelayedAcceptanceNS(ns, step, n_mcmc_steps=T, ring_capacity=100_000,
                                  train_every=200, train_steps=16, batch=256, lr=1e-3,
-                                 bootstrap_steps=600, seed=args.seed)
+                                 bootstrap_steps=600, shift_sigmas=args.shift_sigmas,
+                                 seed=args.seed)
     t0 = time.time()
     drv.bootstrap(torch.cat(dx) if dx else None, torch.cat(dc) if dc else None)
     torch.cuda.synchronize()
@@ -762,6 +763,9 @@ def main():
     ap.add_argument("--cpu-iters", type=int, default=None,
                     help="NS iterations of the CPU samples (default: 2000, 200 for sw)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--shift-sigmas", type=float, default=0.0,
+                    help="sw_da: surrogate contour moved inside by this many robust "
+                         "standard deviations of the surrogate's error")
     ap.add_argument("--no-tune", dest="tune", action="store_false",
                     help="skip jr_autotune (by default it picks the launch shape once, "
                          "after the prologue and outside the timed region)")

@@ -19,8 +19,10 @@
 // 795 (2005)) with the smoothed surrogate constraint
 //   s(x) = sigmoid((emax + contour_shift - H_sur(x)) / tau),
 // H_sur = surrogate U + the exact ensemble term.  Galilean: the trajectory is
-// walked on the surrogate (reflections off its contour, forces only on
-// reflecting steps); stage 1 accepts with min(1, s(x') / s(x)), stage 2
+// walked on the surrogate (reflections off its contour at the inner points,
+// forces only on reflecting steps; the final point does not reflect, which
+// makes the trajectory its own reverse and the proposal symmetric); stage 1
+// accepts with min(1, s(x') / s(x)), stage 2
 // evaluates the exact energy and accepts with 1{E(x') < emax} min(1, s(x) /
 // s(x')).  Volume: stage 1 with min(1, prior ratio s(x') / s(x)) and the exact
 // cell checks, stage 2 as above.  The exact energy decides every step; the
@@ -460,7 +462,12 @@ __device__ __forceinline__ bool da_galilean(const JrParams& P, Walker<G>& w, con
     Hs = sur_ham<false>(w, cidx, ens, sff, sfd);
     ++nsur;
     if (isnan(Hs)) Hs = INFINITY;
-    refl = Hs >= contour;
+    // reflections at the inner points only: the final point never reflects,
+    // so the trajectory retraces itself from (x', -d') back to (x, -d) (the
+    // proposal is symmetric, as delayed acceptance needs); the exact walk
+    // gets this from its acceptance test, which the surrogate trajectory
+    // does not make
+    refl = r + 1 < R && Hs >= contour;
     if (refl) {
       sur_ham<true>(w, cidx, ens, sff, sfd);
       ++nsur;
@@ -468,8 +475,6 @@ __device__ __forceinline__ bool da_galilean(const JrParams& P, Walker<G>& w, con
       coef = __fmul_rn(2.0f * __double2float_rn(sfd), rcp_nr(ffs > 1e-20f ? ffs : 1e-20f));
     }
   }
-  if (refl)
-    for (int q = r0; q < n3; q += gs) arr.dir[q] = __fmaf_rn(-coef, arr.F[q], arr.dir[q]);
   const float ls1 = sur_log_s(Hs, contour, S.tau), ls0 = sur_log_s(Hs0, contour, S.tau);
   const float u1 = uniform01(bits32(split(key.k, 3u), 0u));
   const bool stage1 = logf(u1) < fminf(0.0f, ls1 - ls0);
@@ -545,12 +550,14 @@ __device__ __forceinline__ bool da_volume(const JrParams& P, Walker<G>& w, const
   const double Hs0 = s.Esur;
   const float ls1 = sur_log_s(Hs1, contour, S.tau), ls0 = sur_log_s(Hs0, contour, S.tau);
   // log of min(1, ratio^N) (flat prior: 0)
-  const double pa = volume_prior(ratio, n, mv.flat_v_prior != 0);
+  const double jac = volume_jacobian(ratio, n, mv.flat_v_prior != 0);
   const bool valid = s.cell_ok != 0;
   const float u1 = key.pre ? key.vu : uniform01(bits32(key.k1, 0u));
-  // u1 < min(1, pa s(x') / s(x)); a flat surrogate constraint leaves the
-  // prior test of the exact move
-  const double r1 = pa * exp((double)ls1 - (double)ls0);
+  // u1 < min(1, J s(x') / s(x)) with J = ratio**N the prior ratio (the
+  // first-stage acceptance of delayed acceptance, which the second stage's
+  // min(1, s(x) / s(x')) assumes); a flat surrogate constraint leaves the
+  // prior test of the exact move, u1 < min(1, J)
+  const double r1 = jac * exp((double)ls1 - (double)ls0);
   const bool stage1 = valid && (double)u1 < (r1 < 1.0 ? r1 : 1.0);
   bool acc = false;
   double En = s.E;

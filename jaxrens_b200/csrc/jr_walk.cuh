@@ -1216,9 +1216,9 @@ __device__ inline bool cell_valid(const float* c, int n, const JrMoveParams& mv)
   return (vpa <= mv.max_vpa) && (vpa >= mv.min_vpa) && (amin >= mv.min_aspect);
 }
 
-// Acceptance probability of the volume prior: 1 for a flat prior, else
-// min(1, ratio**N) by lax.integer_pow's binary exponentiation, in float64.
-__device__ __forceinline__ double volume_prior(float ratio, int n, bool flat) {
+// The volume prior's ratio: 1 for a flat prior, else ratio**N by
+// lax.integer_pow's binary exponentiation, in float64.
+__device__ __forceinline__ double volume_jacobian(float ratio, int n, bool flat) {
   if (flat) return 1.0;
   double acc = 1.0, b = (double)ratio;
   bool first = true;
@@ -1231,7 +1231,13 @@ __device__ __forceinline__ double volume_prior(float ratio, int n, bool flat) {
     y >>= 1;
     if (y > 0) b = b * b;
   }
-  return acc < 1.0 ? acc : 1.0;
+  return acc;
+}
+
+// Acceptance probability of the volume prior: min(1, volume_jacobian).
+__device__ __forceinline__ double volume_prior(float ratio, int n, bool flat) {
+  const double j = volume_jacobian(ratio, n, flat);
+  return j < 1.0 ? j : 1.0;
 }
 
 // Volume move (volume.py:49-109 + _common.py:16-93).  Returns acceptance and

@@ -192,7 +192,7 @@ class DelayedAcceptanceNS:
                  n_mcmc_steps: int = 20, ring_capacity: int = 100_000, train_every: int = 50,
                  train_window: int = 100_000, train_steps: int = 16, batch: int = 256,
                  lr: float = 1e-3, warmup_iters: int = 0, bootstrap_steps: int = 200,
-                 margin: float = 0.5, seed: int = 0):
+                 margin: float = 0.5, shift_sigmas: float = 0.0, seed: int = 0):
         import torch
 
         self.ns = ns_state
@@ -208,6 +208,7 @@ class DelayedAcceptanceNS:
         self.lr = float(lr)
         self.warmup_iters = int(warmup_iters)
         self.margin = float(margin)
+        self.shift_sigmas = float(shift_sigmas)
         self.bootstrap_steps = int(bootstrap_steps)
         self.gen = torch.Generator(device=device()).manual_seed(seed)
         self.since_train = 0
@@ -274,8 +275,10 @@ class DelayedAcceptanceNS:
 
     def calibrate(self, idx=None, n: int = 512) -> tuple[float, float]:
         """Set the surrogate constraint from its error d = U_sur - U on
-        recent training configurations: ``contour_shift`` = median(d),
-        ``tau`` = 0.6 x 1.4826 MAD(d) (a logistic of that scale follows the
+        recent training configurations: with sigma = 1.4826 MAD(d),
+        ``contour_shift`` = median(d) - shift_sigmas sigma (a surrogate
+        contour moved inside the true one keeps trajectories inside it more
+        often), ``tau`` = 0.6 sigma (a logistic of that scale follows the
         normal CDF of the error), at least 1e-3.  Either choice leaves the walk
         exact; they set how well stage 1 screens.  Returns (shift, tau)."""
         import torch
@@ -288,9 +291,9 @@ class DelayedAcceptanceNS:
                                         self.ring.cell[idx], forces=False)
         d = Us - self.ring.energy_u[idx]
         med = d.median()
-        mad = (d - med).abs().median()
-        self.sur.contour_shift = float(med)
-        self.sur.tau = max(0.6 * 1.4826 * float(mad), 1e-3)
+        sigma = 1.4826 * float((d - med).abs().median())
+        self.sur.contour_shift = float(med) - self.shift_sigmas * sigma
+        self.sur.tau = max(0.6 * sigma, 1e-3)
         return self.sur.contour_shift, self.sur.tau
 
     def train(self, steps: int, renormalise: bool = False) -> None:
