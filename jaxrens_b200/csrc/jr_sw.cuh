@@ -173,15 +173,22 @@ __device__ __forceinline__ void sw_mask_bits(uint64_t* nbm, bool in, int a, int 
 // segment of q is the number of lanes whose prefix is <= q.
 __device__ __forceinline__ int sw_cand_pair(const uint16_t* cand, int per_warp, int incl,
                                             int nwarps, int q) {
-  int seg = 0, base = 0;
-  for (int l = 0; l < nwarps; ++l) {
-    const int il = __shfl_sync(0xffffffffu, incl, l);
-    if (q >= il) {
-      seg = l + 1;
-      base = il;
+  // the first warp whose inclusive count exceeds q (counts ascend; the last
+  // is M > q), by a binary search of fixed depth so every lane takes part in
+  // every shuffle
+  int lo = 0, hi = nwarps - 1;
+#pragma unroll
+  for (int it = 0; it < 5; ++it) {
+    const int mid = (lo + hi) >> 1;
+    const int v = __shfl_sync(0xffffffffu, incl, mid);
+    if (lo < hi) {
+      if (v > q) hi = mid;
+      else lo = mid + 1;
     }
   }
-  return cand[seg * per_warp + (q - base)];
+  const int below = __shfl_sync(0xffffffffu, incl, lo > 0 ? lo - 1 : 0);
+  const int base = lo > 0 ? below : 0;
+  return cand[lo * per_warp + (q - base)];
 }
 
 // Energy (U) of the walker, forces into arr.F when kForces, and the sums
