@@ -892,7 +892,7 @@ static int move_galilean(const JroModel* mdl, int mode, const uint32_t key[2],
   uint32_t k_init[2], k_pert[2];
   jro_split(key, 0, k_init);
   jro_split(key, 1, k_pert);
-  float* v = (float*)malloc(sizeof(float) * n3);
+  float* v = (float*)calloc((size_t)(n3 > 0 ? n3 : 1), sizeof(float));
   float* x0 = (float*)malloc(sizeof(float) * n3);
   float* dp = (float*)malloc(sizeof(float) * n3);
   double* F = (double*)malloc(sizeof(double) * n3);
