@@ -663,6 +663,55 @@ def _da_arm(name, ns, step, n_steps, walk, torch):
             "mean_contour_after": float(ns.emax.double().mean())}
 
 
+def train_kernel_roofline(drv, torch):
+    """Achieved bfloat16 tensor throughput of one surrogate training step
+    (`jr_sur_train_step`, tcgen05) on the driver's minibatch of ring
+    configurations of 64 atoms (and, beside it, on 4096 configurations):
+    algorithmic flops = 3 x 2 x 5,184 multiply-adds per atom (forward, and a
+    backward of twice the forward) over the batch's atoms, divided by the
+    median CUDA-event duration of 20 steps.  The peak is the measured cuBLAS
+    bf16 figure of the machine when present, else the 1.59 PFLOP/s fallback."""
+    from jaxrens_b200.surrogate import Surrogate
+
+    idx = drv.ring.recent_valid(drv.train_window)
+    N = drv.ring.n_atoms_max
+
+    def step_ms(B):
+        pick = idx[torch.randint(0, idx.numel(), (B,), generator=drv.gen, device=idx.device)]
+        D = Surrogate.descriptors(drv.ring.positions[pick], drv.ring.cell[pick])
+        U = drv.ring.energy_u[pick].contiguous()
+        rows = torch.arange(B, dtype=torch.int32, device=idx.device)
+        times = []
+        for _ in range(20):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            drv.sur.train_step(D, U, rows, 0.0)
+            b.record()
+            b.synchronize()
+            times.append(a.elapsed_time(b))
+        return sorted(times)[len(times) // 2]
+
+    B = drv.batch
+    ms = step_ms(B)
+    ms_big = step_ms(4096)
+    flops = 3 * 2 * 5184 * B * N
+    flops_big = 3 * 2 * 5184 * 4096 * N
+    peak, source = 1590.0, "fallback 1.59 PFLOP/s bf16"
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        try:
+            peak = float(json.load(open(path))["bf16_tflops"])
+            source = "measured (MEASURED_PEAKS.json bf16_tflops)"
+        except (KeyError, ValueError, TypeError):
+            pass
+    achieved = flops / (ms * 1e-3) / 1e12
+    big = flops_big / (ms_big * 1e-3) / 1e12
+    return {"bound": "tensor", "kernel": "sur_train_kernel", "achieved": achieved,
+            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+            "batch": B, "ms_per_step": ms, "flops_per_step": flops, "peak_source": source,
+            "batch_4096": {"achieved": big, "frac": big / peak, "ms_per_step": ms_big}}
+
+
 def run_da(args):
     """The Stillinger-Weber workload walked by delayed acceptance on the
     learned surrogate, beside the exact walk from the same state.  After the
@@ -735,6 +784,7 @@ def run_da(args):
         torch.cuda.synchronize()
         rounds.append((time.perf_counter() - t0) * 1e3)
     train_ms = sorted(rounds)[1]
+    tensor = train_kernel_roofline(drv, torch)
     line = {
         "metric": METRIC, "value": arms[0]["value"], "unit": "walker-steps/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": arms[0]["ms_per_step"],
@@ -747,6 +797,7 @@ def run_da(args):
                       "contour_shift": drv.sur.contour_shift,
                       "tau": drv.sur.tau, "ring_samples": drv.ring.reserved},
         "arms": arms,
+        "roofline": tensor,
         "da_over_exact": arms[0]["value"] / arms[2]["value"],
         "clocks": clk,
     }
