@@ -228,3 +228,15 @@ def test_delayed_acceptance_samples_the_exact_constrained_prior():
         a, b = _np(ie.dead_energy)[row], _np(idd.dead_energy)[row]
         se = np.sqrt(a.var(ddof=1) / P + b.var(ddof=1) / P)
         assert abs(a.mean() - b.mean()) < 4 * se + 1e-9, (row, a, b)
+
+
+def test_energy_only_path_gives_the_same_energy():
+    """The walk's energy-only surrogate evaluation (trajectory steps) and the
+    one with forces (reflections) give the same U bit for bit: both reduce
+    the same per-thread partials by the same tree."""
+    x, c = perturbed_diamond(11, 8)
+    sur = _surrogate_with(6)
+    U0, _ = da.surrogate_energy_forces(sur, x, c, forces=False)
+    U1, F = da.surrogate_energy_forces(sur, x, c, forces=True)
+    np.testing.assert_array_equal(_np(U0), _np(U1))
+    assert np.isfinite(_np(F)).all()
