@@ -360,9 +360,11 @@ typedef struct JrSampleRing {
  * threads) with galilean and volume moves by two-stage delayed acceptance
  * on the surrogate `sur`: stage 1 accepts with the ratio of the smoothed
  * surrogate constraint sigmoid((emax + contour_shift - H_sur) / tau) (galilean
- * trajectories reflect off the surrogate contour; volume moves also take the
- * prior ratio and the cell checks), stage 2 evaluates the exact energy and
- * accepts with 1{E' < emax} times the inverse ratio.  Other moves run as in
+ * trajectories reflect off the surrogate contour at their inner points, never
+ * at the final one, so the proposal is symmetric; volume moves take the
+ * unclamped prior ratio (V'/V)^N times the surrogate ratio and the cell
+ * checks), stage 2 evaluates the exact energy and accepts with
+ * 1{E' < emax} min(1, s(x) / s(x')).  Other moves run as in
  * jr_ns_iterate.  info.n_evaluations counts exact evaluations;
  * ring->n_surrogate_evaluations the surrogate's.  `cfg` may be NULL (the
  * heuristic shape). */
