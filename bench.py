@@ -192,17 +192,28 @@ class ClockSampler:
         self.proc = None
         self.lines: list[str] = []
         self.t = None
+        self.first = 0
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "50"],
+                 "--format=csv,noheader,nounits", "-lms", "10"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi takes a while to print its first line: wait for it so
+            # that a short timed region still falls inside the sampling
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except (OSError, FileNotFoundError):
             self.proc = None
+        self.first = len(self.lines)
+
+    def mark(self) -> None:
+        """The timed region starts now: stop() keeps the samples from here."""
+        self.first = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -218,7 +229,14 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        window = "timed region"
+        lines = self.lines[self.first:]
+        if not lines:
+            # a timed region shorter than the sampling period: the samples
+            # just before it (warm-up steps of the same workload)
+            lines = self.lines[max(0, self.first - 3):]
+            window = "warm-up steps just before the timed region"
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -232,7 +250,7 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": float(max(smax)) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "window": window}
 
 
 def fp32_peak_tflops(torch) -> float:
@@ -338,13 +356,16 @@ def run_ours(args):
         if RE_ON:
             re.apply(ns, step)
 
+    # the clock sampler runs from the warm-up on; its samples from the start
+    # of the timed region are the ones reported
+    clocks = ClockSampler(local)
+    clocks.start()
     for _ in range(args.warmup):
         one_step(None)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
+    clocks.mark()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
